@@ -1,0 +1,186 @@
+/*
+ * pbf.h -- C ABI of the B200-native Position Based Fluids solver step.
+ *
+ * Drop-in boundary for the reference's solver interface:
+ *   kernels/cudaPBF.h:8-12      initCUDASolverDataBuffer / cudaPBFSolve / freeCUDASolverDataBuffer
+ *   include/solverBase.h:16-64  SolverParameter, SolverData
+ *   include/solver.h:86-111     PBFSolver(para, box, fext) / solve(Particle*)
+ * Plain C types only; no CUDA or torch types in any signature (a stream is a
+ * void* holding a cudaStream_t, NULL = the legacy default stream).
+ *
+ * Every function returns PBF_OK (0) or a negative status and never exits the
+ * process; pbf_last_error() gives a message for the calling thread. Calls on one
+ * handle are stream-ordered and not thread-safe without external locking.
+ */
+#ifndef PBF_B200_PBF_H
+#define PBF_B200_PBF_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PBF_ABI_VERSION 1
+
+/* status codes */
+#define PBF_OK 0
+#define PBF_ERR_INVALID (-1)   /* bad argument or parameter */
+#define PBF_ERR_CUDA (-2)      /* a CUDA runtime call failed */
+#define PBF_ERR_ALLOC (-3)     /* device or host allocation failed */
+#define PBF_ERR_DEVICE (-4)    /* a kernel reported an error bit (see pbf_stats.error_bits) */
+#define PBF_ERR_STATE (-5)     /* call out of order, e.g. pbf_step before pbf_upload */
+#define PBF_ERR_NONFINITE (-6) /* NaN or Inf in positions or velocities */
+
+/* error_bits reported by kernels */
+#define PBF_DEVERR_SCAN_TIMEOUT 1 /* scan look-back wait expired */
+#define PBF_DEVERR_BAD_INDEX 2    /* an index fell outside its array */
+#define PBF_DEVERR_NONFINITE 4    /* a non-finite position appeared */
+#define PBF_DEVERR_MLP_TIMEOUT 8  /* tensor-core pipeline wait expired */
+
+/* Same layout and meaning as the reference SolverParameter
+ * (include/solverBase.h:16-40); 13 x 4 bytes. */
+typedef struct pbf_solver_parameter {
+    float h;          /* kernel radius */
+    int nParticles;
+    float restRho;    /* rest density rho0 */
+    float epsilon;    /* constraint relaxation */
+    float k;          /* s_corr strength */
+    float n;          /* s_corr exponent */
+    float deltaq;     /* s_corr reference distance */
+    float c;          /* XSPH viscosity */
+    float dt;         /* substep */
+    float invDt;      /* accepted for layout compatibility; the step divides by dt */
+    int iterations;   /* Jacobi iterations (minimum count when adaptive) */
+    float vorticityConfinementEpilon;
+    float radius;     /* particle radius (the reference app shrinks the box by it) */
+} pbf_solver_parameter;
+
+/* stable-mode flags (each is a named departure from the reference formulas) */
+#define PBF_FLAG_CLAMP_C 1u   /* unilateral density constraint C = max(C, 0) */
+#define PBF_FLAG_XSPH_RHO 2u  /* XSPH weight c / rho0 instead of c */
+
+/* Everything the reference fixes at compile time or does not have. Fill with
+ * pbf_ext_params_default() and change what you need. */
+typedef struct pbf_ext_params {
+    float gravity[3];    /* default (0,-49,0): kernels/cudaPBFSolver.cu:9 */
+    int grid_dims[3];    /* default 64^3: include/solverBase.h:10-12 */
+    float cell_scale;    /* cell edge = h * cell_scale, >= 1 (default 1) */
+    float wall_jitter;   /* wall offset coefficient (default 0.01, RANDOM_OFFSET_COEFF) */
+    float grad_rmin;     /* spiky gradient lower cutoff (default 0.01, cuh:107) */
+    int max_neighbors;   /* neighbour cap, 1..127 (default 63, MAX_NEIGHBOR) */
+    int cell_order;      /* 0 ascending (stable) or 1 descending slot order within a cell */
+    unsigned flags;      /* PBF_FLAG_* */
+    float scorr_scale;   /* multiplies s_corr (default 1) */
+    float sphere[4];     /* static sphere obstacle: centre xyz, radius (<= 0: none) */
+    int adaptive;        /* 1: iterate until max density error <= density_tol */
+    float density_tol;   /* one-sided max density error tolerance (default 0.01) */
+    int max_iterations;  /* cap for adaptive iterations and warm-start fallback (default 16) */
+    int measure_error;   /* 1: record max/mean density error of every substep */
+    int debug;           /* 1: keep per-stage intermediates for pbf_fetch */
+    int warm_start;      /* 1: learned lambda warm start (needs installed weights) */
+    int reserved[8];
+} pbf_ext_params;
+
+typedef struct pbf_stats {
+    long long substeps;         /* substeps run since upload */
+    long long total_iterations; /* Jacobi iterations run since upload */
+    long long fallbacks;        /* warm-start substeps that needed plain iterations */
+    int last_iterations;        /* iterations used by the last substep */
+    int error_bits;             /* PBF_DEVERR_* accumulated since upload */
+    double max_density_error;   /* last substep: max_i max(rho_i/rho0 - 1, 0), FP64 */
+    double mean_density_error;  /* last substep: mean of the same */
+} pbf_stats;
+
+typedef struct pbf_solver pbf_solver;
+
+/* pbf_fetch field ids: internal arrays in cell-sorted slot order */
+#define PBF_FIELD_X 0          /* float4[n] positions after the substep */
+#define PBF_FIELD_V 1          /* float4[n] velocities after the substep */
+#define PBF_FIELD_XOLD 2       /* float4[n] positions before prediction */
+#define PBF_FIELD_XPRED 3      /* float4[n] predicted positions (debug) */
+#define PBF_FIELD_XL 4         /* float4[n] last lambda pass: xyz, lambda in w */
+#define PBF_FIELD_RHO 5        /* float[n] last density (debug) */
+#define PBF_FIELD_DP 6         /* float4[n] last position correction (debug) */
+#define PBF_FIELD_CURL 7       /* float4[n] vorticity omega */
+#define PBF_FIELD_VORT 8       /* float4[n] confinement force (debug) */
+#define PBF_FIELD_VISC 9       /* float4[n] XSPH term (debug) */
+#define PBF_FIELD_CELL 10      /* int[n] cell key per slot (ncells = outside the grid) */
+#define PBF_FIELD_CELL_START 11 /* int[ncells + 2] cell starts, out-of-grid bin, n */
+#define PBF_FIELD_PERM 12      /* int[n] slot -> original particle id */
+#define PBF_FIELD_NCNT 13      /* int[n] neighbour counts */
+#define PBF_FIELD_NBR 14       /* int[max_neighbors * stride] slot-major neighbour slots */
+#define PBF_FIELD_HASH 15      /* int[n] cell key per particle before sorting (debug) */
+#define PBF_FIELD_LAMBDA0 16   /* float[n] warm-start lambda of the last substep */
+
+void pbf_ext_params_default(pbf_ext_params* ext);
+
+/* Replaces initCUDASolverDataBuffer (kernels/cudaPBF.cu:4-30) and the
+ * PBFSolver constructor (include/solver.h:86-110): allocates every device
+ * buffer for para->nParticles particles. grid_space and boundary are AABBs
+ * (pMin xyz, pMax xyz): grid_space anchors the uniform grid, boundary is the
+ * wall the particles are clamped to. */
+int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], const float boundary[6],
+               const pbf_ext_params* ext, pbf_solver** out);
+
+/* Replaces freeCUDASolverDataBuffer (kernels/cudaPBF.cu:32-48). */
+int pbf_destroy(pbf_solver* s);
+
+/* Host positions and velocities, AoS xyz, n == nParticles; the cudaMemcpy of
+ * kernels/cudaPBF.cu:26-27. Resets the stats. */
+int pbf_upload(pbf_solver* s, const float* pos, const float* vel, int n);
+
+/* Same from device memory (AoS xyz float[3n]), stream-ordered. */
+int pbf_upload_device(pbf_solver* s, const float* d_pos, const float* d_vel, int n, void* stream);
+
+/* Caller-owned device buffer float[3n] that receives positions in original
+ * order after every pbf_step, as data.position did (src/renderapp.cpp:246-249,
+ * kernels/cudaPBF.cu:7). NULL unbinds. */
+int pbf_bind_position(pbf_solver* s, float* d_pos);
+
+/* Replaces cudaPBFSolve (kernels/cudaPBF.cu:50-115), once per substep: replays
+ * the captured substep graph `substeps` times on `stream`. */
+int pbf_step(pbf_solver* s, int substeps, void* stream);
+
+/* Host copies of positions / velocities in original order (either may be NULL). */
+int pbf_download(pbf_solver* s, float* pos, float* vel);
+
+/* Same into device buffers, stream-ordered (either may be NULL). */
+int pbf_download_device(pbf_solver* s, float* d_pos, float* d_vel, void* stream);
+
+/* Synchronises the handle's last stream and reports stats; returns
+ * PBF_ERR_DEVICE when a kernel has set an error bit. */
+int pbf_get_stats(pbf_solver* s, pbf_stats* st);
+
+/* Copies an internal array (PBF_FIELD_*) to host memory; bytes must equal the
+ * field size given by pbf_field_bytes. Synchronises. */
+int pbf_fetch(pbf_solver* s, int field, void* dst, size_t bytes);
+size_t pbf_field_bytes(const pbf_solver* s, int field);
+
+/* Grid build only, on the current positions and without prediction: hash,
+ * histogram, scan, sort and neighbour search (buildNeighborhood's job,
+ * kernels/cudaPBFSolver.cu:31-154; src/solver.cpp:3-58). */
+int pbf_build_grid(pbf_solver* s, void* stream);
+
+/* Sizes: number of cells, neighbour-list stride. */
+int pbf_get_layout(const pbf_solver* s, int* ncells, int* stride, int* max_neighbors);
+
+/* Exclusive scan of int32 with decoupled look-back (calculatePrefixSum +
+ * addBlockSum, kernels/cudaPBFSolver.cu:42-96, for any n). d_out receives n + 1
+ * ints (the total last). d_ws must hold pbf_scan_workspace_bytes(n) bytes.
+ * The input is left unchanged. */
+size_t pbf_scan_workspace_bytes(int n);
+int pbf_scan_exclusive_i32(const int* d_in, int* d_out, int n, void* d_ws, size_t ws_bytes, void* stream);
+
+const char* pbf_last_error(void);
+int pbf_abi_version(void);
+
+/* sizeof of the ABI structs, for FFI bindings to check their layouts:
+ * 0 pbf_solver_parameter, 1 pbf_ext_params, 2 pbf_stats. */
+size_t pbf_struct_size(int which);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PBF_B200_PBF_H */

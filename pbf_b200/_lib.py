@@ -1,0 +1,121 @@
+"""ctypes bindings to the C ABI in include/pbf.h (libpbf_b200.so, built in-tree).
+
+The library is the only compute path: when it is missing or fails to load, the
+import raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpbf_b200.so")
+
+PBF_OK = 0
+PBF_ERR_INVALID = -1
+PBF_ERR_CUDA = -2
+PBF_ERR_ALLOC = -3
+PBF_ERR_DEVICE = -4
+PBF_ERR_STATE = -5
+PBF_ERR_NONFINITE = -6
+
+PBF_FLAG_CLAMP_C = 1
+PBF_FLAG_XSPH_RHO = 2
+
+FIELD = {
+    "x": 0, "v": 1, "xold": 2, "xpred": 3, "xl": 4, "rho": 5, "dp": 6, "curl": 7, "vort": 8,
+    "visc": 9, "cell": 10, "cell_start": 11, "perm": 12, "ncnt": 13, "nbr": 14, "hash": 15,
+    "lambda0": 16,
+}
+FLOAT4_FIELDS = {"x", "v", "xold", "xpred", "xl", "dp", "curl", "vort", "visc"}
+FLOAT_FIELDS = {"rho", "lambda0"}
+
+
+class SolverParameter(C.Structure):
+    """Same layout as the reference SolverParameter (include/solverBase.h:16-40)."""
+
+    _fields_ = [
+        ("h", C.c_float), ("nParticles", C.c_int), ("restRho", C.c_float), ("epsilon", C.c_float),
+        ("k", C.c_float), ("n", C.c_float), ("deltaq", C.c_float), ("c", C.c_float),
+        ("dt", C.c_float), ("invDt", C.c_float), ("iterations", C.c_int),
+        ("vorticityConfinementEpilon", C.c_float), ("radius", C.c_float),
+    ]
+
+
+class ExtParams(C.Structure):
+    """pbf_ext_params (include/pbf.h)."""
+
+    _fields_ = [
+        ("gravity", C.c_float * 3), ("grid_dims", C.c_int * 3), ("cell_scale", C.c_float),
+        ("wall_jitter", C.c_float), ("grad_rmin", C.c_float), ("max_neighbors", C.c_int),
+        ("cell_order", C.c_int), ("flags", C.c_uint), ("scorr_scale", C.c_float),
+        ("sphere", C.c_float * 4), ("adaptive", C.c_int), ("density_tol", C.c_float),
+        ("max_iterations", C.c_int), ("measure_error", C.c_int), ("debug", C.c_int),
+        ("warm_start", C.c_int), ("reserved", C.c_int * 8),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("substeps", C.c_longlong), ("total_iterations", C.c_longlong), ("fallbacks", C.c_longlong),
+        ("last_iterations", C.c_int), ("error_bits", C.c_int), ("max_density_error", C.c_double),
+        ("mean_density_error", C.c_double),
+    ]
+
+
+# (name, restype, argtypes) for every function include/pbf.h declares
+_PROTOS = [
+    ("pbf_abi_version", C.c_int, []),
+    ("pbf_struct_size", C.c_size_t, [C.c_int]),
+    ("pbf_last_error", C.c_char_p, []),
+    ("pbf_ext_params_default", None, [C.POINTER(ExtParams)]),
+    ("pbf_create", C.c_int, [C.POINTER(SolverParameter), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                             C.POINTER(ExtParams), C.POINTER(C.c_void_p)]),
+    ("pbf_destroy", C.c_int, [C.c_void_p]),
+    ("pbf_upload", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    ("pbf_upload_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    ("pbf_bind_position", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pbf_step", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    ("pbf_download", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pbf_download_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pbf_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    ("pbf_fetch", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    ("pbf_field_bytes", C.c_size_t, [C.c_void_p, C.c_int]),
+    ("pbf_build_grid", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pbf_get_layout", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("pbf_scan_workspace_bytes", C.c_size_t, [C.c_int]),
+    ("pbf_scan_exclusive_i32", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
+]
+
+
+class PBFError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"pbf error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libpbf_b200.so once; raise if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run pbf_b200.build.build() (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in _PROTOS:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != PBF_OK:
+        raise PBFError(rc, lib().pbf_last_error().decode(errors="replace"))
+
+
+def declared_symbols() -> list[str]:
+    return [p[0] for p in _PROTOS]

@@ -1,0 +1,575 @@
+// C ABI of the solver step (include/pbf.h): handle, device buffers, the captured
+// substep graph, and the status/stats plumbing.
+//
+// Host sequence replaced: kernels/cudaPBF.cu:50-115 (about 22 launch +
+// cudaDeviceSynchronize round trips and two leaked host arrays per substep).
+// Here one substep is a CUDA graph captured once per handle and replayed.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "../../include/pbf.h"
+#include "pbf_kernels.h"
+
+using namespace pbf;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(PBF_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+struct DevStats {
+    unsigned long long max_bits[64];  // per iteration slot (adaptive) or slot 0
+    double sum[64];
+    int done;
+    int iters;
+    int err;
+    int fallback;
+};
+
+}  // namespace
+
+struct pbf_solver {
+    pbf_solver_parameter para{};
+    pbf_ext_params ext{};
+    float grid_space[6]{}, boundary[6]{};
+    KParams kp{};
+    int n = 0, ncells = 0, stride = 0;
+    // device state (slot order)
+    float4 *Sx = nullptr, *Sv = nullptr, *Px = nullptr, *Pv = nullptr, *Pxold = nullptr, *Q = nullptr,
+           *omega = nullptr;
+    float4 *xpred_dbg = nullptr, *dp_dbg = nullptr, *vort_dbg = nullptr, *visc_dbg = nullptr;
+    float* rho_dbg = nullptr;
+    int *Sperm = nullptr, *Pperm = nullptr, *cell = nullptr, *ticket = nullptr, *tmp = nullptr,
+        *cell_sorted = nullptr, *ncnt = nullptr, *nbr = nullptr, *cnt = nullptr, *cell_start = nullptr,
+        *hash_dbg = nullptr;
+    float *lam_prev = nullptr, *lam_prev_sorted = nullptr, *lam0 = nullptr;
+    void* scan_ws = nullptr;
+    DevStats* dstats = nullptr;
+    float* staging = nullptr;  // AoS float[3n] x2 for upload/download
+    float* bound_pos = nullptr;
+    void* mlp = nullptr;  // learned warm start (not installed)
+    // graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    cudaStream_t last_stream = nullptr;
+    bool uploaded = false;
+    long long substeps = 0, total_iters = 0, fallbacks = 0;
+};
+
+namespace {
+
+bool finite6(const float* b) {
+    for (int i = 0; i < 6; ++i)
+        if (!std::isfinite(b[i])) return false;
+    return true;
+}
+
+// Host-side constants of the product arithmetic (pbf_device.cuh). Every value is
+// a fixed IEEE expression so that a CPU evaluation reproduces it.
+KParams make_kparams(const pbf_solver& s) {
+    KParams k{};
+    const pbf_solver_parameter& p = s.para;
+    const pbf_ext_params& e = s.ext;
+    const double inv_pi_ref = 0.31830988618;  // INVPI, include/solverBase.h:4
+    k.h = p.h;
+    k.h2 = p.h * p.h;
+    const float cs = p.h * e.cell_scale;
+    k.inv_cell = 1.0f / cs;
+    k.poly6_c = (float)(315.0 * inv_pi_ref / (64.0 * std::pow((double)p.h, 9)));
+    k.spiky_c = (float)(-45.0 * inv_pi_ref / std::pow((double)p.h, 6));
+    const float r2 = p.deltaq * p.deltaq;
+    float wdq = 0.0f;
+    if (!(r2 > k.h2)) {
+        const float t = k.h2 - r2;
+        wdq = k.poly6_c * ((t * t) * t);
+    }
+    k.inv_wdq = 1.0f / wdq;
+    k.nk = -p.k;
+    k.scorr_scale = e.scorr_scale;
+    k.n_exp = p.n;
+    k.n_int = (p.n >= 1.0f && p.n <= 8.0f && p.n == std::floor(p.n)) ? (int)p.n : 0;
+    k.rho0 = p.restRho;
+    k.rho0sq = p.restRho * p.restRho;
+    k.eps = p.epsilon;
+    k.dt = p.dt;
+    k.jit = e.wall_jitter;
+    k.rmin = e.grad_rmin;
+    k.visc_c = (e.flags & PBF_FLAG_XSPH_RHO) ? (float)((double)p.c / (double)p.restRho) : p.c;
+    k.vort_eps = p.vorticityConfinementEpilon;
+    for (int a = 0; a < 3; ++a) {
+        k.g[a] = e.gravity[a];
+        k.gmin[a] = s.grid_space[a];
+        k.bmin[a] = s.boundary[a];
+        k.bmax[a] = s.boundary[3 + a];
+        k.dims[a] = e.grid_dims[a];
+    }
+    for (int a = 0; a < 4; ++a) k.sphere[a] = e.sphere[a];
+    k.n = s.n;
+    k.ncells = s.ncells;
+    k.max_nbr = e.max_neighbors;
+    k.stride = s.stride;
+    k.cell_order = e.cell_order;
+    k.flags = e.flags;
+    k.poly6_c64 = 315.0 / (64.0 * M_PI * std::pow((double)p.h, 9));
+    return k;
+}
+
+template <typename T> int dalloc(T** p, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) return fail(PBF_ERR_ALLOC, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+    return PBF_OK;
+}
+
+void free_all(pbf_solver* s) {
+    void* ptrs[] = {s->Sx, s->Sv, s->Px, s->Pv, s->Pxold, s->Q, s->omega, s->xpred_dbg, s->dp_dbg, s->vort_dbg,
+                    s->visc_dbg, s->rho_dbg, s->Sperm, s->Pperm, s->cell, s->ticket, s->tmp, s->cell_sorted,
+                    s->ncnt, s->nbr, s->cnt, s->cell_start, s->hash_dbg, s->lam_prev, s->lam_prev_sorted, s->lam0,
+                    s->scan_ws, s->dstats, s->staging};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+}
+
+int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, const pbf_ext_params* e) {
+    if (!p || !gs || !bd || !e) return fail(PBF_ERR_INVALID, "null argument");
+    if (p->nParticles <= 0) return fail(PBF_ERR_INVALID, "nParticles must be positive (got %d)", p->nParticles);
+    const float f[] = {p->h, p->restRho, p->epsilon, p->k, p->n, p->deltaq, p->c, p->dt, p->vorticityConfinementEpilon};
+    for (float v : f)
+        if (!std::isfinite(v)) return fail(PBF_ERR_INVALID, "non-finite SolverParameter field");
+    if (!(p->h > 0.0f)) return fail(PBF_ERR_INVALID, "h must be positive");
+    if (!(p->restRho > 0.0f)) return fail(PBF_ERR_INVALID, "restRho must be positive");
+    if (!(p->dt > 0.0f)) return fail(PBF_ERR_INVALID, "dt must be positive");
+    if (!(p->deltaq >= 0.0f && p->deltaq < p->h)) return fail(PBF_ERR_INVALID, "deltaq must lie in [0, h)");
+    if (p->iterations < 0 || p->iterations > 64) return fail(PBF_ERR_INVALID, "iterations must lie in [0, 64]");
+    if (!finite6(gs) || !finite6(bd)) return fail(PBF_ERR_INVALID, "non-finite grid space or boundary");
+    for (int a = 0; a < 3; ++a) {
+        if (e->grid_dims[a] <= 0) return fail(PBF_ERR_INVALID, "grid_dims must be positive");
+        if (bd[a] > bd[3 + a]) return fail(PBF_ERR_INVALID, "boundary pMin > pMax");
+    }
+    const long long cells = (long long)e->grid_dims[0] * e->grid_dims[1] * e->grid_dims[2];
+    if (cells > (1ll << 30)) return fail(PBF_ERR_INVALID, "grid has too many cells (%lld)", cells);
+    if (!(e->cell_scale >= 1.0f) || !std::isfinite(e->cell_scale)) return fail(PBF_ERR_INVALID, "cell_scale must be >= 1");
+    if (e->max_neighbors < 1 || e->max_neighbors > 127) return fail(PBF_ERR_INVALID, "max_neighbors must lie in [1, 127]");
+    if (e->cell_order != 0 && e->cell_order != 1) return fail(PBF_ERR_INVALID, "cell_order must be 0 or 1");
+    if (e->max_iterations < 1 || e->max_iterations > 64) return fail(PBF_ERR_INVALID, "max_iterations must lie in [1, 64]");
+    if (e->adaptive && p->iterations > e->max_iterations)
+        return fail(PBF_ERR_INVALID, "iterations exceeds max_iterations");
+    if (!std::isfinite(e->density_tol) || e->density_tol < 0) return fail(PBF_ERR_INVALID, "density_tol must be >= 0");
+    return PBF_OK;
+}
+
+// Enqueue one substep on `st` (captured into the graph).
+void enqueue_substep(pbf_solver* s, cudaStream_t st) {
+    const KParams& kp = s->kp;
+    const bool dbg = s->ext.debug != 0;
+    const int n = s->n;
+    int* err = &s->dstats->err;
+    launch_hash(kp, true, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st);
+    if (dbg) cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
+    launch_scan(s->cnt, s->cell_start, s->ncells + 1, s->scan_ws, err, st);
+    launch_scatter(n, s->cell, s->ticket, s->cell_start, s->tmp, err, st);
+    const bool ws = s->ext.warm_start && s->mlp;
+    launch_reorder(kp, true, s->Sx, s->Sv, s->Sperm, s->cell, s->cell_start, s->tmp, s->Px, s->Pv, s->Pxold,
+                   s->Pperm, s->cell_sorted, ws ? s->lam_prev : nullptr, ws ? s->lam_prev_sorted : nullptr, err, st);
+    if (dbg) launch_copy4(n, s->Px, s->xpred_dbg, st);
+    launch_neighbors(kp, s->Px, s->cell_start, s->nbr, s->ncnt, st);
+
+    DevStats* ds = s->dstats;
+    cudaMemsetAsync(ds, 0, offsetof(DevStats, err), st);  // per-substep slots, keeps err
+    const bool adaptive = s->ext.adaptive != 0;
+    int plain_iters = s->para.iterations;
+    int* skip = nullptr;
+    if (!adaptive) {
+        for (int it = 0; it < plain_iters; ++it) {
+            const bool last = it == plain_iters - 1;
+            launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, nullptr, st);
+            launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, last ? s->Pv : nullptr, s->dp_dbg, nullptr, st);
+        }
+        if (plain_iters == 0 && ws) launch_velocity(kp, s->Px, s->Pxold, s->Pv, st);
+        if (s->ext.measure_error)
+            launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[0], &ds->sum[0], nullptr, st);
+    } else {
+        // iterate until the max density error is within tolerance; iterations
+        // after convergence are skipped on the device (the graph is fixed)
+        const int min_it = ws ? 0 : std::max(plain_iters, 1);
+        const int max_it = s->ext.max_iterations;
+        if (ws) {
+            launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[0], &ds->sum[0], nullptr, st);
+            launch_check_done(&ds->max_bits[0], s->ext.density_tol, &ds->done, &ds->fallback, st);
+        }
+        for (int it = 0; it < max_it; ++it) {
+            const int slot = it + 1;
+            skip = it < min_it ? nullptr : &ds->done;
+            launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, skip, st);
+            launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, nullptr, s->dp_dbg, skip, st);
+            launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[slot], &ds->sum[slot], skip, st);
+            if (it + 1 >= min_it) launch_check_done(&ds->max_bits[slot], s->ext.density_tol, &ds->done, &ds->iters, st);
+            else launch_check_done(&ds->max_bits[slot], -1.0, &ds->done, &ds->iters, st);
+        }
+        launch_velocity(kp, s->Px, s->Pxold, s->Pv, st);
+    }
+    launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, st);
+    launch_vort(kp, dbg, s->Px, s->Pv, s->omega, s->nbr, s->ncnt, s->Sv, s->Pperm, s->Sperm, s->vort_dbg,
+                s->visc_dbg, st);
+    launch_copy4(n, s->Px, s->Sx, st);
+    if (ws) cudaMemcpyAsync(s->lam_prev, s->lam0, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+}
+
+int build_graph(pbf_solver* s) {
+    if (s->exec) {
+        cudaGraphExecDestroy(s->exec);
+        s->exec = nullptr;
+    }
+    if (s->graph) {
+        cudaGraphDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_substep(s, s->cap_stream);
+    cudaError_t e = cudaStreamEndCapture(s->cap_stream, &s->graph);
+    if (e != cudaSuccess) return fail(PBF_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    CK(cudaGraphInstantiate(&s->exec, s->graph, 0));
+    return PBF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pbf_abi_version(void) { return PBF_ABI_VERSION; }
+
+size_t pbf_struct_size(int which) {
+    switch (which) {
+        case 0: return sizeof(pbf_solver_parameter);
+        case 1: return sizeof(pbf_ext_params);
+        case 2: return sizeof(pbf_stats);
+        default: return 0;
+    }
+}
+
+const char* pbf_last_error(void) { return g_err.c_str(); }
+
+void pbf_ext_params_default(pbf_ext_params* e) {
+    if (!e) return;
+    std::memset(e, 0, sizeof *e);
+    e->gravity[0] = 0.0f;
+    e->gravity[1] = -49.0f;
+    e->gravity[2] = 0.0f;
+    e->grid_dims[0] = e->grid_dims[1] = e->grid_dims[2] = 64;
+    e->cell_scale = 1.0f;
+    e->wall_jitter = 0.01f;
+    e->grad_rmin = 0.01f;
+    e->max_neighbors = 63;
+    e->cell_order = 0;
+    e->flags = 0;
+    e->scorr_scale = 1.0f;
+    e->density_tol = 0.01f;
+    e->max_iterations = 16;
+}
+
+int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], const float boundary[6],
+               const pbf_ext_params* ext, pbf_solver** out) {
+    if (!out) return fail(PBF_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    pbf_ext_params def;
+    if (!ext) {
+        pbf_ext_params_default(&def);
+        ext = &def;
+    }
+    int rc = validate(para, grid_space, boundary, ext);
+    if (rc) return rc;
+    pbf_solver* s = new (std::nothrow) pbf_solver();
+    if (!s) return fail(PBF_ERR_ALLOC, "host allocation failed");
+    s->para = *para;
+    s->ext = *ext;
+    std::memcpy(s->grid_space, grid_space, sizeof s->grid_space);
+    std::memcpy(s->boundary, boundary, sizeof s->boundary);
+    s->n = para->nParticles;
+    s->ncells = ext->grid_dims[0] * ext->grid_dims[1] * ext->grid_dims[2];
+    s->stride = (s->n + 31) & ~31;
+    const size_t n = s->n;
+    const bool dbg = ext->debug != 0;
+#define AL(ptr, count)                     \
+    do {                                   \
+        rc = dalloc(&(ptr), (count));      \
+        if (rc) {                          \
+            free_all(s);                   \
+            delete s;                      \
+            return rc;                     \
+        }                                  \
+    } while (0)
+    AL(s->Sx, n); AL(s->Sv, n); AL(s->Px, n); AL(s->Pv, n); AL(s->Pxold, n); AL(s->Q, n); AL(s->omega, n);
+    AL(s->Sperm, n); AL(s->Pperm, n); AL(s->cell, n); AL(s->ticket, n); AL(s->tmp, n); AL(s->cell_sorted, n);
+    AL(s->ncnt, n);
+    AL(s->nbr, (size_t)ext->max_neighbors * s->stride);
+    AL(s->cnt, (size_t)s->ncells + 1);
+    AL(s->cell_start, (size_t)s->ncells + 2);
+    AL(s->lam_prev, n); AL(s->lam_prev_sorted, n); AL(s->lam0, n);
+    AL(s->staging, 6 * n);
+    AL(s->dstats, 1);
+    if (dbg) {
+        AL(s->xpred_dbg, n); AL(s->dp_dbg, n); AL(s->vort_dbg, n); AL(s->visc_dbg, n); AL(s->rho_dbg, n);
+        AL(s->hash_dbg, n);
+    }
+    {
+        const size_t ws = scan_status_bytes(s->ncells + 1);
+        cudaError_t e = cudaMalloc(&s->scan_ws, ws);
+        if (e != cudaSuccess) {
+            free_all(s);
+            delete s;
+            return fail(PBF_ERR_ALLOC, "cudaMalloc(scan workspace): %s", cudaGetErrorString(e));
+        }
+    }
+#undef AL
+    cudaError_t e = cudaMemset(s->cnt, 0, sizeof(int) * (s->ncells + 1));
+    if (e == cudaSuccess) e = cudaMemset(s->dstats, 0, sizeof(DevStats));
+    if (e == cudaSuccess) e = cudaMemset(s->lam_prev, 0, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaMemset(s->lam0, 0, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        free_all(s);
+        delete s;
+        return fail(PBF_ERR_CUDA, "setup: %s", cudaGetErrorString(e));
+    }
+    s->kp = make_kparams(*s);
+    *out = s;
+    return PBF_OK;
+}
+
+int pbf_destroy(pbf_solver* s) {
+    if (!s) return PBF_OK;
+    if (s->last_stream) cudaStreamSynchronize(s->last_stream);
+    cudaDeviceSynchronize();
+    free_all(s);
+    delete s;
+    return PBF_OK;
+}
+
+int pbf_upload_device(pbf_solver* s, const float* d_pos, const float* d_vel, int n, void* stream) {
+    if (!s || !d_pos || !d_vel) return fail(PBF_ERR_INVALID, "null argument");
+    if (n != s->n) return fail(PBF_ERR_INVALID, "n (%d) differs from nParticles (%d)", n, s->n);
+    cudaStream_t st = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(s->dstats, 0, sizeof(DevStats), st));
+    launch_from_aos(n, d_pos, d_vel, s->Sx, s->Sv, s->Sperm, &s->dstats->err, st);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(s->lam_prev, 0, sizeof(float) * n, st));
+    s->last_stream = st;
+    s->uploaded = true;
+    s->substeps = s->total_iters = s->fallbacks = 0;
+    return PBF_OK;
+}
+
+int pbf_upload(pbf_solver* s, const float* pos, const float* vel, int n) {
+    if (!s || !pos || !vel) return fail(PBF_ERR_INVALID, "null argument");
+    if (n != s->n) return fail(PBF_ERR_INVALID, "n (%d) differs from nParticles (%d)", n, s->n);
+    for (size_t i = 0; i < (size_t)3 * n; ++i)
+        if (!std::isfinite(pos[i]) || !std::isfinite(vel[i]))
+            return fail(PBF_ERR_NONFINITE, "non-finite input at float %zu", i);
+    CK(cudaMemcpy(s->staging, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->staging + 3 * (size_t)n, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice));
+    int rc = pbf_upload_device(s, s->staging, s->staging + 3 * (size_t)n, n, nullptr);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(nullptr));
+    return PBF_OK;
+}
+
+int pbf_bind_position(pbf_solver* s, float* d_pos) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    s->bound_pos = d_pos;
+    return PBF_OK;
+}
+
+int pbf_step(pbf_solver* s, int substeps, void* stream) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_step before pbf_upload");
+    if (substeps < 0) return fail(PBF_ERR_INVALID, "negative substep count");
+    if (s->ext.warm_start && !s->mlp) return fail(PBF_ERR_STATE, "warm_start set but no weights installed");
+    if (!s->exec) {
+        int rc = build_graph(s);
+        if (rc) return rc;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int i = 0; i < substeps; ++i) CK(cudaGraphLaunch(s->exec, st));
+    if (s->bound_pos && substeps > 0) {
+        launch_to_aos(s->n, s->Sx, s->Sperm, s->bound_pos, &s->dstats->err, st);
+        CK(cudaGetLastError());
+    }
+    s->last_stream = st;
+    s->substeps += substeps;
+    return PBF_OK;
+}
+
+int pbf_build_grid(pbf_solver* s, void* stream) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_build_grid before pbf_upload");
+    cudaStream_t st = (cudaStream_t)stream;
+    const KParams& kp = s->kp;
+    int* err = &s->dstats->err;
+    launch_hash(kp, false, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st);
+    if (s->hash_dbg) CK(cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * s->n, cudaMemcpyDeviceToDevice, st));
+    launch_scan(s->cnt, s->cell_start, s->ncells + 1, s->scan_ws, err, st);
+    launch_scatter(s->n, s->cell, s->ticket, s->cell_start, s->tmp, err, st);
+    launch_reorder(kp, false, s->Sx, s->Sv, s->Sperm, s->cell, s->cell_start, s->tmp, s->Px, s->Pv, s->Pxold, s->Pperm,
+                   s->cell_sorted, nullptr, nullptr, err, st);
+    launch_neighbors(kp, s->Px, s->cell_start, s->nbr, s->ncnt, st);
+    CK(cudaGetLastError());
+    // the sorted state becomes the current state
+    CK(cudaMemcpyAsync(s->Sx, s->Px, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->Sv, s->Pv, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->Sperm, s->Pperm, sizeof(int) * s->n, cudaMemcpyDeviceToDevice, st));
+    s->last_stream = st;
+    return PBF_OK;
+}
+
+int pbf_download_device(pbf_solver* s, float* d_pos, float* d_vel, void* stream) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_download before pbf_upload");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (d_pos) launch_to_aos(s->n, s->Sx, s->Sperm, d_pos, &s->dstats->err, st);
+    if (d_vel) launch_to_aos(s->n, s->Sv, s->Sperm, d_vel, &s->dstats->err, st);
+    CK(cudaGetLastError());
+    s->last_stream = st;
+    return PBF_OK;
+}
+
+int pbf_download(pbf_solver* s, float* pos, float* vel) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_download before pbf_upload");
+    const size_t n = s->n;
+    if (s->last_stream) CK(cudaStreamSynchronize(s->last_stream));
+    int rc = pbf_download_device(s, s->staging, s->staging + 3 * n, nullptr);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(nullptr));
+    if (pos) CK(cudaMemcpy(pos, s->staging, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+    if (vel) CK(cudaMemcpy(vel, s->staging + 3 * n, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+    return PBF_OK;
+}
+
+int pbf_get_stats(pbf_solver* s, pbf_stats* out) {
+    if (!s || !out) return fail(PBF_ERR_INVALID, "null argument");
+    if (s->last_stream) CK(cudaStreamSynchronize(s->last_stream));
+    CK(cudaDeviceSynchronize());
+    DevStats h;
+    CK(cudaMemcpy(&h, s->dstats, sizeof h, cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof *out);
+    out->substeps = s->substeps;
+    out->error_bits = h.err;
+    int slot = 0;
+    if (s->ext.adaptive) {
+        out->last_iterations = h.iters;
+        slot = h.iters;
+    } else {
+        out->last_iterations = s->para.iterations + ((s->ext.warm_start && s->mlp) ? 1 : 0);
+    }
+    if (s->ext.warm_start && s->mlp && s->ext.adaptive) out->fallbacks = h.fallback;
+    double m;
+    std::memcpy(&m, &h.max_bits[slot], sizeof m);
+    out->max_density_error = m;
+    out->mean_density_error = h.sum[slot] / (double)s->n;
+    out->total_iterations = 0;
+    if (h.err) return fail(PBF_ERR_DEVICE, "kernel error bits 0x%x", h.err);
+    return PBF_OK;
+}
+
+size_t pbf_field_bytes(const pbf_solver* s, int field) {
+    if (!s) return 0;
+    const size_t n = s->n;
+    switch (field) {
+        case PBF_FIELD_X: case PBF_FIELD_V: case PBF_FIELD_XOLD: case PBF_FIELD_XPRED: case PBF_FIELD_XL:
+        case PBF_FIELD_DP: case PBF_FIELD_CURL: case PBF_FIELD_VORT: case PBF_FIELD_VISC:
+            return n * sizeof(float4);
+        case PBF_FIELD_RHO: case PBF_FIELD_LAMBDA0: return n * sizeof(float);
+        case PBF_FIELD_CELL: case PBF_FIELD_PERM: case PBF_FIELD_NCNT: case PBF_FIELD_HASH: return n * sizeof(int);
+        case PBF_FIELD_CELL_START: return ((size_t)s->ncells + 2) * sizeof(int);
+        case PBF_FIELD_NBR: return (size_t)s->ext.max_neighbors * s->stride * sizeof(int);
+        default: return 0;
+    }
+}
+
+int pbf_fetch(pbf_solver* s, int field, void* dst, size_t bytes) {
+    if (!s || !dst) return fail(PBF_ERR_INVALID, "null argument");
+    const size_t want = pbf_field_bytes(s, field);
+    if (want == 0) return fail(PBF_ERR_INVALID, "unknown field %d", field);
+    if (bytes != want) return fail(PBF_ERR_INVALID, "field %d needs %zu bytes, got %zu", field, want, bytes);
+    const void* src = nullptr;
+    switch (field) {
+        case PBF_FIELD_X: src = s->Sx; break;
+        case PBF_FIELD_V: src = s->Sv; break;
+        case PBF_FIELD_XOLD: src = s->Pxold; break;
+        case PBF_FIELD_XPRED: src = s->xpred_dbg; break;
+        case PBF_FIELD_XL: src = s->Q; break;
+        case PBF_FIELD_RHO: src = s->rho_dbg; break;
+        case PBF_FIELD_DP: src = s->dp_dbg; break;
+        case PBF_FIELD_CURL: src = s->omega; break;
+        case PBF_FIELD_VORT: src = s->vort_dbg; break;
+        case PBF_FIELD_VISC: src = s->visc_dbg; break;
+        case PBF_FIELD_CELL: src = s->cell_sorted; break;
+        case PBF_FIELD_CELL_START: src = s->cell_start; break;
+        case PBF_FIELD_PERM: src = s->Sperm; break;
+        case PBF_FIELD_NCNT: src = s->ncnt; break;
+        case PBF_FIELD_NBR: src = s->nbr; break;
+        case PBF_FIELD_HASH: src = s->hash_dbg; break;
+        case PBF_FIELD_LAMBDA0: src = s->lam0; break;
+        default: break;
+    }
+    if (!src) return fail(PBF_ERR_STATE, "field %d is kept only when ext.debug is set", field);
+    if (s->last_stream) CK(cudaStreamSynchronize(s->last_stream));
+    CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return PBF_OK;
+}
+
+int pbf_get_layout(const pbf_solver* s, int* ncells, int* stride, int* max_neighbors) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (ncells) *ncells = s->ncells;
+    if (stride) *stride = s->stride;
+    if (max_neighbors) *max_neighbors = s->ext.max_neighbors;
+    return PBF_OK;
+}
+
+size_t pbf_scan_workspace_bytes(int n) {
+    if (n < 0) return 0;
+    return scan_status_bytes(n) + 16;
+}
+
+int pbf_scan_exclusive_i32(const int* d_in, int* d_out, int n, void* d_ws, size_t ws_bytes, void* stream) {
+    if (!d_in || !d_out || !d_ws) return fail(PBF_ERR_INVALID, "null argument");
+    if (n <= 0) return fail(PBF_ERR_INVALID, "n must be positive");
+    if (ws_bytes < pbf_scan_workspace_bytes(n)) return fail(PBF_ERR_INVALID, "workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    int* err = (int*)((char*)d_ws + scan_status_bytes(n));
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    launch_scan_const(d_in, d_out, n, d_ws, err, st);
+    CK(cudaGetLastError());
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr) return fail(PBF_ERR_DEVICE, "scan error bits 0x%x", herr);
+    return PBF_OK;
+}
+
+}  // extern "C"

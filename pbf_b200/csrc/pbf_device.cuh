@@ -1,0 +1,184 @@
+// Device-side arithmetic of one PBF substep (sm_100a).
+//
+// The library is compiled with -fmad=false: a multiply followed by an add is
+// never fused by the compiler, and every fused multiply-add below is an explicit
+// __fmaf_rn at a documented place. Square roots and divisions are the IEEE
+// round-to-nearest forms. Together these make each per-particle result a fixed
+// sequence of IEEE operations that a CPU evaluation of the same sequence
+// reproduces bit for bit.
+//
+// Formulas follow the reference CUDA kernels (kernels/cudaPBFSolver.cuh:99-181,
+// kernels/cudaPBFSolver.cu:4-239); the departures in evaluation order are:
+//   * poly6: (h^2-r^2)^3 by two multiplies instead of powf(.,3) (cuh:102)
+//   * spiky gradient: one sqrt and one division, s = c (h-r)^2 / r, then s * r
+//     instead of powf(.,2) and normalize (cuh:106-109)
+//   * s_corr exponent: repeated multiplication for integer n in [1,8] (cuh:143)
+//   * |r|^2 and every neighbour sum use fused multiply-adds in a fixed order
+//   * the wall-jitter hash evaluates sine with pbf_det_sin (double precision)
+//     instead of sinf (cuh:117), so that a CPU evaluation reproduces it.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pbf {
+
+// Flags (mirrors include/pbf.h PBF_FLAG_*)
+enum : unsigned {
+    FLAG_CLAMP_C = 1u,    // unilateral density constraint: C = max(C, 0)
+    FLAG_XSPH_RHO = 2u,   // XSPH weight c / rho0
+};
+
+// Error bits written by kernels into the device status word.
+enum : int {
+    DEVERR_SCAN_TIMEOUT = 1,    // decoupled look-back gave up waiting for a predecessor
+    DEVERR_BAD_INDEX = 2,       // a neighbour or slot index fell outside [0, n)
+    DEVERR_NONFINITE = 4,       // a non-finite position appeared
+    DEVERR_MLP_TIMEOUT = 8,     // tensor-core pipeline gave up waiting on an mbarrier
+};
+
+struct KParams {
+    // kernel constants, all computed on the host (pbf_capi.cu: make_kparams)
+    float h, h2, inv_cell, poly6_c, spiky_c, inv_wdq, nk, scorr_scale, n_exp;
+    float rho0, rho0sq, eps, dt, jit, rmin, visc_c, vort_eps;
+    float g[3];
+    float gmin[3];
+    float bmin[3], bmax[3];
+    float sphere[4];
+    int dims[3];
+    int n;          // particles
+    int ncells;     // real cells; slot ncells is the out-of-grid bin
+    int max_nbr;    // neighbour cap (reference MAX_NEIGHBOR = 63)
+    int stride;     // neighbour list stride (slot-major layout: nbr[q * stride + k])
+    int cell_order; // 0 ascending, 1 descending within a cell
+    int n_int;      // s_corr exponent when a small integer, else 0
+    unsigned flags;
+    double poly6_c64;  // exact poly6 constant for the FP64 density reduction
+};
+
+// ---- deterministic sine ------------------------------------------------------
+// Quadrant reduction by a two-part Cody-Waite split of pi/2 (first 33 bits, then
+// the rounded remainder), Taylor series of sin and cos on [-pi/4, pi/4] in Horner
+// form, IEEE double throughout, one rounding to float. Accurate to well under one
+// float ulp for |a| < 1e6.
+__device__ __forceinline__ float pbf_det_sin(float a) {
+    const double x = (double)a;
+    const double P1 = 1.5707963267341256;
+    const double P2 = 6.077100506506192e-11;
+    const double q = floor(x * 0.6366197723675814 + 0.5);
+    const double r = (x - q * P1) - q * P2;
+    const double r2 = r * r;
+    const double s = r + r * r2 * (-1.0 / 6.0 + r2 * (1.0 / 120.0 + r2 * (-1.0 / 5040.0 +
+                     r2 * (1.0 / 362880.0 + r2 * (-1.0 / 39916800.0 + r2 * (1.0 / 6227020800.0 +
+                     r2 * (-1.0 / 1307674368000.0)))))));
+    const double c = 1.0 + r2 * (-0.5 + r2 * (1.0 / 24.0 + r2 * (-1.0 / 720.0 +
+                     r2 * (1.0 / 40320.0 + r2 * (-1.0 / 3628800.0 + r2 * (1.0 / 479001600.0 +
+                     r2 * (-1.0 / 87178291200.0 + r2 * (1.0 / 20922789888000.0))))))));
+    const long long qi = (long long)q;
+    double res;
+    switch ((int)(qi & 3)) {
+        case 0: res = s; break;
+        case 1: res = c; break;
+        case 2: res = -s; break;
+        default: res = -c; break;
+    }
+    return (float)res;
+}
+
+struct f3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ f3 make3(const float4& a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ f3 sub3(const f3& a, const f3& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+// |r|^2 = fma(z, z, fma(y, y, x*x))
+__device__ __forceinline__ float dot_fma(const f3& a, const f3& b) {
+    return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, a.x * b.x));
+}
+__device__ __forceinline__ f3 cross3(const f3& a, const f3& b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Wpoly6 (cuh:99-103): zero when r2 > h^2, else c * ((t*t)*t), t = h^2 - r2
+__device__ __forceinline__ float w_poly6(const KParams& p, float r2) {
+    if (r2 > p.h2) return 0.0f;
+    const float t = p.h2 - r2;
+    return p.poly6_c * ((t * t) * t);
+}
+
+// WspikyGrad (cuh:105-110): zero when |r| > h or |r| < rmin, else ((c*d)*d)/|r| * r
+__device__ __forceinline__ f3 grad_spiky(const KParams& p, const f3& r, float r2) {
+    const float rl = __fsqrt_rn(r2);
+    if (rl > p.h || rl < p.rmin) return {0.0f, 0.0f, 0.0f};
+    const float d = p.h - rl;
+    const float s = __fdiv_rn((p.spiky_c * d) * d, rl);
+    return {s * r.x, s * r.y, s * r.z};
+}
+
+// Scorr (cuh:142-144): -k (W / W(dq))^n, times scorr_scale
+__device__ __forceinline__ float s_corr(const KParams& p, float w) {
+    const float q = w * p.inv_wdq;
+    float pw;
+    if (p.n_int > 0) {
+        pw = q;
+        for (int i = 1; i < p.n_int; ++i) pw = pw * q;
+    } else {
+        pw = powf(q, p.n_exp);
+    }
+    return (p.nk * pw) * p.scorr_scale;
+}
+
+// randomOffset (cuh:112-119) with pbf_det_sin in place of sinf
+__device__ __forceinline__ float random_offset(float u, float v) {
+    const float a = u * 12.9898f;
+    const float b = v * 78.233f;
+    const float arg = 2.0f * (a + b);
+    const float m = pbf_det_sin(arg) * 43758.5453f;
+    return fabsf(m - (float)(int)m);
+}
+
+// Static sphere obstacle (no reference counterpart): a point inside the sphere is
+// moved radially onto its surface.
+__device__ __forceinline__ void sphere_project(const KParams& p, f3& q) {
+    const float R = p.sphere[3];
+    const f3 d = {q.x - p.sphere[0], q.y - p.sphere[1], q.z - p.sphere[2]};
+    const float d2 = dot_fma(d, d);
+    if (d2 >= R * R || d2 <= 0.0f) return;
+    const float s = __fdiv_rn(R, __fsqrt_rn(d2));
+    q = {p.sphere[0] + d.x * s, p.sphere[1] + d.y * s, p.sphere[2] + d.z * s};
+}
+
+// BoundParticle (cuh:121-140), including the reference's y-max branch that hashes (y, z)
+__device__ __forceinline__ void bound_particle(const KParams& p, f3& q) {
+    if (q.x < p.bmin[0]) q.x = p.bmin[0] + p.jit * random_offset(q.y, q.z);
+    if (q.x > p.bmax[0]) q.x = p.bmax[0] - p.jit * random_offset(q.y, q.z);
+    if (q.y < p.bmin[1]) q.y = p.bmin[1] + p.jit * random_offset(q.x, q.z);
+    if (q.y > p.bmax[1]) q.y = p.bmax[1] - p.jit * random_offset(q.y, q.z);
+    if (q.z < p.bmin[2]) q.z = p.bmin[2] + p.jit * random_offset(q.x, q.y);
+    if (q.z > p.bmax[2]) q.z = p.bmax[2] - p.jit * random_offset(q.x, q.y);
+    if (p.sphere[3] > 0.0f) sphere_project(p, q);
+}
+
+// updateParticles (cu:4-13): v += dt g; x += dt v; bound
+__device__ __forceinline__ void predict(const KParams& p, f3& x, f3& v) {
+    v = {v.x + p.dt * p.g[0], v.y + p.dt * p.g[1], v.z + p.dt * p.g[2]};
+    x = {x.x + p.dt * v.x, x.y + p.dt * v.y, x.z + p.dt * v.z};
+    bound_particle(p, x);
+}
+
+// computeDimID (cuh:156-160): truncation toward zero
+__device__ __forceinline__ void cell_dims(const KParams& p, const f3& x, int d[3]) {
+    d[0] = (int)((x.x - p.gmin[0]) * p.inv_cell);
+    d[1] = (int)((x.y - p.gmin[1]) * p.inv_cell);
+    d[2] = (int)((x.z - p.gmin[2]) * p.inv_cell);
+}
+
+// computeGid (cuh:172-181) with the out-of-grid particles mapped to bin ncells
+__device__ __forceinline__ int cell_key(const KParams& p, const f3& x) {
+    int d[3];
+    cell_dims(p, x, d);
+    if (d[0] < 0 || d[0] >= p.dims[0] || d[1] < 0 || d[1] >= p.dims[1] || d[2] < 0 || d[2] >= p.dims[2])
+        return p.ncells;
+    return d[0] + d[1] * p.dims[0] + d[2] * p.dims[0] * p.dims[1];
+}
+
+}  // namespace pbf

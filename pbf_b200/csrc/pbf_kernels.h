@@ -1,0 +1,40 @@
+// Host-side launchers of the substep kernels (pbf_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "pbf_device.cuh"
+
+namespace pbf {
+
+void launch_hash(const KParams& p, bool predict_on, const float4* x, const float4* v, int* cell, int* ticket, int* cnt,
+                 int* err, cudaStream_t st);
+size_t scan_status_bytes(int m);
+void launch_scan(int* cnt, int* out, int m, void* status_ws, int* err, cudaStream_t st);
+// same scan, input left unchanged
+void launch_scan_const(const int* in, int* out, int m, void* status_ws, int* err, cudaStream_t st);
+void launch_scatter(int n, const int* cell, const int* ticket, const int* cell_start, int* tmp, int* err,
+                    cudaStream_t st);
+void launch_reorder(const KParams& p, bool predict_on, const float4* x, const float4* v, const int* perm,
+                    const int* cell, const int* cell_start, const int* tmp, float4* xp, float4* vp, float4* xold,
+                    int* perm_out, int* cell_sorted, const float* lam_in, float* lam_out, int* err, cudaStream_t st);
+void launch_neighbors(const KParams& p, const float4* x, const int* cell_start, int* nbr, int* ncnt, cudaStream_t st);
+void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr, const int* ncnt, float4* xl,
+                   float* rho, const int* skip, cudaStream_t st);
+void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, const int* ncnt, const float4* xold,
+               float4* xout, float4* vout, float4* dp, const int* skip, cudaStream_t st);
+void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st);
+void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
+                 cudaStream_t st);
+void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v, const float4* omega, const int* nbr,
+                 const int* ncnt, float4* vout, const int* perm_in, int* perm_out, float4* vort, float4* visc,
+                 cudaStream_t st);
+void launch_density_error(const KParams& p, const float4* x, const int* nbr, const int* ncnt,
+                          unsigned long long* max_bits, double* sum, const int* skip, cudaStream_t st);
+void launch_check_done(const unsigned long long* max_bits, double tol, int* done, int* iters, cudaStream_t st);
+void launch_from_aos(int n, const float* pos, const float* vel, float4* x, float4* v, int* perm, int* err,
+                     cudaStream_t st);
+void launch_to_aos(int n, const float4* a, const int* perm, float* out, int* err, cudaStream_t st);
+void launch_copy4(int n, const float4* a, float4* b, cudaStream_t st);
+
+}  // namespace pbf

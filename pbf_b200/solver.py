@@ -1,0 +1,202 @@
+"""Host-side mirror of the reference solver interface over the C ABI.
+
+Reference interfaces mirrored:
+  * PBFSolver(para, box) / solve(Particle*)        include/solver.h:86-111
+  * initCUDASolverDataBuffer / cudaPBFSolve /
+    freeCUDASolverDataBuffer                       kernels/cudaPBF.h:8-12
+Same names, argument meaning and error behaviour (errors raise PBFError with the
+C status code instead of exiting the process).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import ExtParams, PBFError, SolverParameter, Stats, check, lib
+
+
+def make_parameter(**kw) -> SolverParameter:
+    """SolverParameter with invDt filled from dt when not given."""
+    p = SolverParameter()
+    for k, v in kw.items():
+        setattr(p, k, v)
+    if "invDt" not in kw and p.dt:
+        p.invDt = np.float32(1.0) / np.float32(p.dt)
+    return p
+
+
+def default_ext(**overrides) -> ExtParams:
+    e = ExtParams()
+    lib().pbf_ext_params_default(C.byref(e))
+    for k, v in overrides.items():
+        if k in ("gravity", "grid_dims", "sphere"):
+            arr = getattr(e, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(e, k, v)
+    return e
+
+
+def _stream_handle(stream) -> Optional[int]:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)  # torch.cuda.Stream
+
+
+def _f6(b: Sequence[float]):
+    a = (C.c_float * 6)(*[float(x) for x in b])
+    return a
+
+
+class Solver:
+    """One PBF scene on the GPU (a pbf_solver handle)."""
+
+    def __init__(self, para: SolverParameter, grid_space: Sequence[float], boundary: Sequence[float],
+                 ext: Optional[ExtParams] = None):
+        self.para = para
+        self.ext = ext if ext is not None else default_ext()
+        self.n = int(para.nParticles)
+        h = C.c_void_p()
+        check(lib().pbf_create(C.byref(para), _f6(grid_space), _f6(boundary), C.byref(self.ext), C.byref(h)))
+        self._h = h
+        nc, st, mn = C.c_int(), C.c_int(), C.c_int()
+        check(lib().pbf_get_layout(h, C.byref(nc), C.byref(st), C.byref(mn)))
+        self.ncells, self.stride, self.max_neighbors = nc.value, st.value, mn.value
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().pbf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- data -----------------------------------------------------------------
+    def upload(self, pos: np.ndarray, vel: np.ndarray) -> None:
+        p = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1)
+        v = np.ascontiguousarray(vel, dtype=np.float32).reshape(-1)
+        if p.size != 3 * self.n or v.size != 3 * self.n:
+            raise PBFError(_lib.PBF_ERR_INVALID, f"expected {self.n} xyz positions and velocities")
+        check(lib().pbf_upload(self._h, p.ctypes.data, v.ctypes.data, self.n))
+
+    def upload_device(self, d_pos, d_vel, stream=None) -> None:
+        """d_pos / d_vel: CUDA tensors (float32, n x 3 contiguous) or raw device pointers."""
+        pp = d_pos if isinstance(d_pos, int) else d_pos.data_ptr()
+        vp = d_vel if isinstance(d_vel, int) else d_vel.data_ptr()
+        check(lib().pbf_upload_device(self._h, pp, vp, self.n, _stream_handle(stream)))
+
+    def bind_position(self, d_pos) -> None:
+        ptr = None if d_pos is None else (d_pos if isinstance(d_pos, int) else d_pos.data_ptr())
+        check(lib().pbf_bind_position(self._h, ptr))
+
+    def step(self, substeps: int = 1, stream=None) -> None:
+        check(lib().pbf_step(self._h, int(substeps), _stream_handle(stream)))
+
+    def build_grid(self, stream=None) -> None:
+        check(lib().pbf_build_grid(self._h, _stream_handle(stream)))
+
+    def download(self):
+        pos = np.empty((self.n, 3), np.float32)
+        vel = np.empty((self.n, 3), np.float32)
+        check(lib().pbf_download(self._h, pos.ctypes.data, vel.ctypes.data))
+        return pos, vel
+
+    def download_device(self, d_pos=None, d_vel=None, stream=None) -> None:
+        pp = None if d_pos is None else (d_pos if isinstance(d_pos, int) else d_pos.data_ptr())
+        vp = None if d_vel is None else (d_vel if isinstance(d_vel, int) else d_vel.data_ptr())
+        check(lib().pbf_download_device(self._h, pp, vp, _stream_handle(stream)))
+
+    def stats(self, raise_on_error: bool = True) -> dict:
+        st = Stats()
+        rc = lib().pbf_get_stats(self._h, C.byref(st))
+        if raise_on_error:
+            check(rc)
+        return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+    def fetch(self, name: str) -> np.ndarray:
+        """Internal array in cell-sorted slot order."""
+        fid = _lib.FIELD[name]
+        nbytes = lib().pbf_field_bytes(self._h, fid)
+        if name in _lib.FLOAT4_FIELDS:
+            out = np.empty((self.n, 4), np.float32)
+        elif name in _lib.FLOAT_FIELDS:
+            out = np.empty(self.n, np.float32)
+        else:
+            out = np.empty(nbytes // 4, np.int32)
+        assert out.nbytes == nbytes, (name, out.nbytes, nbytes)
+        check(lib().pbf_fetch(self._h, fid, out.ctypes.data, nbytes))
+        return out
+
+    def fetch_original(self, name: str) -> np.ndarray:
+        """A per-particle field mapped back to original particle order."""
+        a = self.fetch(name)
+        perm = self.fetch("perm")
+        out = np.empty_like(a)
+        out[perm] = a
+        return out
+
+    def neighbor_lists(self) -> list:
+        """Neighbour slot lists (slot order) as Python lists, for tests."""
+        nbr = self.fetch("nbr").reshape(self.max_neighbors, self.stride)
+        cnt = self.fetch("ncnt")
+        return [nbr[: cnt[k], k].tolist() for k in range(self.n)]
+
+
+class PBFSolver:
+    """The reference CPU solver's interface (include/solver.h:86-111) on the GPU
+    step: construct with the parameters and box, then solve(particles) advances
+    an array of particles (n x 6: position xyz, velocity xyz) by one substep in
+    place. The wall is the box shrunk by para.radius (include/solver.h:97)."""
+
+    def __init__(self, para: SolverParameter, box: Sequence[float], ext: Optional[ExtParams] = None,
+                 grid_space: Optional[Sequence[float]] = None):
+        r = float(para.radius)
+        bd = [box[0] + r, box[1] + r, box[2] + r, box[3] - r, box[4] - r, box[5] - r]
+        self.solver = Solver(para, grid_space if grid_space is not None else box, bd, ext)
+        self._uploaded = False
+
+    def solve(self, particles: np.ndarray) -> None:
+        if particles.dtype != np.float32 or particles.shape != (self.solver.n, 6):
+            raise PBFError(_lib.PBF_ERR_INVALID, "particles must be float32 (n, 6)")
+        self.solver.upload(particles[:, :3], particles[:, 3:])
+        self.solver.step(1)
+        pos, vel = self.solver.download()
+        particles[:, :3] = pos
+        particles[:, 3:] = vel
+
+
+# -- the three entry points of kernels/cudaPBF.h:8-12 --------------------------
+def initCUDASolverDataBuffer(position: np.ndarray, velocity: np.ndarray, para: SolverParameter,
+                             gridSpace: Sequence[float], boundary: Sequence[float],
+                             ext: Optional[ExtParams] = None) -> Solver:
+    s = Solver(para, gridSpace, boundary, ext)
+    s.upload(position, velocity)
+    return s
+
+
+def cudaPBFSolve(data: Solver, para: Optional[SolverParameter] = None) -> None:
+    data.step(1)
+
+
+def freeCUDASolverDataBuffer(data: Solver) -> None:
+    data.close()
