@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark: particle-substeps/s of the PBF solver step on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one step = one PBF substep): the 262,144-particle dam break (64^3
+lattice at spacing 0.5h with +-0.01h seeded jitter, h = 0.1, box 80h x 40h x
+40h, rest density 6378, eps 600, s_corr k 0.1 n 4 dq 0.2h, XSPH 0.01,
+vorticity 0.0005, dt = 1/120, 4 Jacobi iterations), synthetic data.
+
+Timing: W untimed substeps, then K substeps, each bracketed by CUDA events on
+the launching stream after an L2 flush (a 256 MiB write); value = particles x K
+/ sum of substep times, whole job (max over ranks). Under torchrun every rank
+runs its own replica of the scene (no data-path collective).
+
+--impl reference times the reference's own CPU solver (src/solver.cpp built
+from its sources into oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "particle-substeps/s at ≤1% max density error: plain vs learned+batched, 1×B200"
+UNIT = "particle-substeps/s"
+L2_FLUSH_BYTES = 256 << 20
+# algorithmic bytes per particle and launch (12-byte vectors, each array read or written once)
+ALG_BYTES = {"hash": 16, "reorder": 80, "lambda": 16, "dp": 28, "curl": 36, "vort": 48, "neighbors": 12}
+# algorithmic flops per neighbour pair (FMA = 2)
+ALG_FLOPS_PER_PAIR = {"lambda": 30, "dp": 40, "curl": 25, "vort": 30}
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured", p
+    return 6650.0, "fallback", {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self) -> dict:
+        if not self.proc or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(seconds: float = 12.0) -> dict:
+    """The reference CPU solver (kind "reference"), or the oracle port when the
+    reference could not be built, on a bounded sample: the 32^3 corner block of
+    the dam break (32,768 particles, same parameters), substeps until `seconds`."""
+    from oracle import oracle as O
+    from pbf_b200 import scenes
+    sc = scenes.dam_break(32, (80, 40, 40), stable=False)
+    if O.refcpu_available():
+        ref = O.RefCpu(sc.para, sc.grid_space, dims=(80, 40, 40))
+        threads = os.cpu_count() or 1
+        ref.set_threads(threads)
+        pos, vel = sc.pos, sc.vel
+        steps, t0 = 0, time.perf_counter()
+        while True:
+            pos, vel = ref.solve(pos, vel, substeps=1, quiet=True)
+            steps += 1
+            el = time.perf_counter() - t0
+            if el >= seconds or steps >= 200:
+                break
+        return {"value": sc.n * steps / el, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"reference PBFSolver::solve (src/solver.cpp, -O3 -fopenmp, stdout to /dev/null), "
+                          f"{steps} substeps of the 32^3 block (32,768 particles) of the dam break, "
+                          f"grid 80x40x40, {el:.1f} s"}
+    orc = O.Oracle(O.params_for_scene(sc, arith=1), sc.pos, sc.vel)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        orc.substep()
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 200:
+            break
+    return {"value": sc.n * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle port, {steps} substeps of the 32^3 block (32,768 particles), {el:.1f} s"}
+
+
+def run_reference(args) -> int:
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from pbf_b200 import scenes
+    sc = scenes.dam_break(32, (80, 40, 40), stable=False)
+    line = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "impl": "reference", "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args)}
+    if not O.refcpu_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver not built (oracle/_ref missing)"}))
+        return 0
+    ref = O.RefCpu(sc.para, sc.grid_space, dims=(80, 40, 40))
+    threads = os.cpu_count() or 1
+    ref.set_threads(threads)
+    pos, vel = sc.pos, sc.vel
+    for _ in range(args.warmup):
+        pos, vel = ref.solve(pos, vel, substeps=1, quiet=True)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        pos, vel = ref.solve(pos, vel, substeps=1, quiet=True)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    v = sc.n * args.steps / tot
+    line.update({"value": v, "ms_per_step": 1e3 * tot / args.steps, "vs_baseline": None,
+                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                                  "sample": "each step one reference PBFSolver::solve (src/solver.cpp, -O3 "
+                                            "-fopenmp, stdout to /dev/null) of the 32^3 block (32,768 particles) "
+                                            "of the dam break, grid 80x40x40"},
+                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line))
+    return 0
+
+
+def workload_config(args) -> dict:
+    return {"workload": "dam_break_262144: 64^3 lattice, spacing 0.5h, jitter 0.01h, h=0.1, box 80h x 40h x 40h, "
+                        "rho0 6378, eps 600, 4 Jacobi iterations, dt 1/120, stable mode",
+            "particles": 262144, "iterations": 4, "grid": [80, 40, 40],
+            "l2": "flushed before every timed step (256 MiB write)",
+            "parallelism": f"{args.gpus} independent replicas" if args.gpus > 1 else "single scene"}
+
+
+def run_b200(args) -> int:
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import pbf_b200
+    from pbf_b200 import Solver, scenes
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sc = scenes.config1(seed=rank, iterations=4)
+    n = sc.n
+    stream = torch.cuda.current_stream()
+    solver = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(profile=1))
+    solver.upload(sc.pos, sc.vel)
+    kernels = solver.kernel_count()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    for _ in range(max(args.warmup, 3)):
+        solver.step(1, stream)
+    torch.cuda.synchronize()
+
+    stage_acc = {}
+    errs = []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            solver.step(1, stream)
+            ev[k][1].record(stream)
+            torch.cuda.synchronize()
+            for name, ms in solver.stage_times().items():
+                stage_acc[name] = stage_acc.get(name, 0.0) + ms
+            errs.append(solver.measure_density_error(stream))
+        torch.cuda.synchronize()
+    barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    tot_s = max_over_ranks(sum(step_ms) / 1e3)
+    value = n * world * args.steps / tot_s
+    stages = {k: v / args.steps for k, v in stage_acc.items() if v > 0}
+    ncnt = solver.fetch("ncnt")
+    pairs = float(ncnt.sum())
+
+    # L2-warm throughput: the same substeps back to back without flushing
+    warm = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    warm[0].record(stream)
+    solver.step(args.steps, stream)
+    warm[1].record(stream)
+    torch.cuda.synchronize()
+    warm_s = max_over_ranks(warm[0].elapsed_time(warm[1]) / 1e3)
+
+    # end to end through the public API: pinned host state in, step, positions out
+    pos_h, vel_h = solver.download()
+    pin_pos = torch.from_numpy(pos_h).pin_memory()
+    pin_vel = torch.from_numpy(vel_h).pin_memory()
+    out_h = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    d_pos = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    d_vel = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    d_out = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        e2e_ev[k][0].record(stream)
+        d_pos.copy_(pin_pos, non_blocking=True)
+        d_vel.copy_(pin_vel, non_blocking=True)
+        solver.upload_device(d_pos, d_vel, stream)
+        solver.step(1, stream)
+        solver.download_device(d_out, None, stream)
+        out_h.copy_(d_out, non_blocking=True)
+        e2e_ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev) / 1e3)
+    e2e_value = n * world * args.steps / e2e_s
+
+    hbm_peak, peak_kind, mp = peaks()
+    dom = max(("lambda", "dp", "neighbors", "curl", "vort"), key=lambda s: stages.get(s, 0.0))
+    per_launch = {"lambda": 4, "dp": 4}.get(dom, 1)
+    launch_ms = stages[dom] / per_launch
+    alg_bytes = ALG_BYTES[dom] * n
+    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
+    traffic = load_traffic(dom)
+    fp32_peak = 148 * 128 * 2 * (mp.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    flops = ALG_FLOPS_PER_PAIR.get(dom, 0) * pairs
+    step_bytes = (283.8 + 44 * 4) * n
+    clocks = clk.summary()
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * tot_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered lattice)",
+        "config": workload_config(args),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 12 * n,
+                "note": "pinned host positions+velocities in, upload, one substep, positions out, every step"},
+        "gpu_launches": kernels * args.steps,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "alg_bytes_per_launch": alg_bytes, "launch_ms": launch_ms},
+        "roofline_fp32": {"kernel": dom, "achieved": flops / (launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                          "peak": fp32_peak, "frac": flops / (launch_ms * 1e-3) / 1e12 / fp32_peak,
+                          "peak_kind": "nominal 148 SM x 128 lanes x 2 at sm_max_mhz", "pairs": pairs},
+        "roofline_step": {"alg_bytes_per_step": step_bytes, "achieved_gbs": step_bytes / (tot_s / args.steps) / 1e9,
+                          "frac_hbm": step_bytes / (tot_s / args.steps) / 1e9 / hbm_peak},
+        "stages_ms": {k: round(v, 5) for k, v in stages.items()},
+        "value_l2_warm": n * world * args.steps / warm_s,
+        "density_error": {"max": max(e[0] for e in errs), "mean": statistics.mean(e[1] for e in errs),
+                          "target_max": 0.01, "meets_target": max(e[0] for e in errs) <= 0.01},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1:
+        out["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(out))
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def load_traffic(kernel: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    return t.get(kernel, {}).get("dram_bytes_per_launch")
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

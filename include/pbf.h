@@ -59,6 +59,7 @@ typedef struct pbf_solver_parameter {
 /* stable-mode flags (each is a named departure from the reference formulas) */
 #define PBF_FLAG_CLAMP_C 1u   /* unilateral density constraint C = max(C, 0) */
 #define PBF_FLAG_XSPH_RHO 2u  /* XSPH weight c / rho0 instead of c */
+#define PBF_FLAG_WALL_DENSITY 4u /* boundary faces add the density of a fluid half-space */
 
 /* Everything the reference fixes at compile time or does not have. Fill with
  * pbf_ext_params_default() and change what you need. */
@@ -79,7 +80,8 @@ typedef struct pbf_ext_params {
     int measure_error;   /* 1: record max/mean density error of every substep */
     int debug;           /* 1: keep per-stage intermediates for pbf_fetch */
     int warm_start;      /* 1: learned lambda warm start (needs installed weights) */
-    int reserved[8];
+    int profile;         /* 1: time every launch with CUDA events (pbf_stage_times) */
+    int reserved[7];
 } pbf_ext_params;
 
 typedef struct pbf_stats {
@@ -164,6 +166,22 @@ int pbf_build_grid(pbf_solver* s, void* stream);
 
 /* Sizes: number of cells, neighbour-list stride. */
 int pbf_get_layout(const pbf_solver* s, int* ncells, int* stride, int* max_neighbors);
+
+/* Profiling (ext.profile = 1): milliseconds per stage in the last substep, summed
+ * over the launches of each stage. Stages: 0 hash, 1 scan, 2 scatter,
+ * 3 reorder, 4 neighbours, 5 lambda, 6 dp, 7 velocity, 8 curl, 9 vorticity,
+ * 10 copy, 11 density measurement, 12 warm-start MLP. */
+#define PBF_NUM_STAGES 13
+int pbf_stage_times(pbf_solver* s, float* ms, int nstages);
+
+/* Number of kernel launches in one substep (kernel nodes of the substep graph);
+ * negative status on error. */
+int pbf_graph_kernel_count(pbf_solver* s);
+
+/* One-sided density error max_i max(rho_i/rho0 - 1, 0) and its mean over the
+ * current positions (FP64 accumulation over each neighbour list); synchronises
+ * `stream`. */
+int pbf_measure_density_error(pbf_solver* s, double* max_err, double* mean_err, void* stream);
 
 /* Exclusive scan of int32 with decoupled look-back (calculatePrefixSum +
  * addBlockSum, kernels/cudaPBFSolver.cu:42-96, for any n). d_out receives n + 1

@@ -59,6 +59,7 @@ typedef struct oracle_params {
 enum {
     ORACLE_CLAMP_C = 1,      // unilateral density constraint C = max(C, 0)
     ORACLE_XSPH_RHO = 2,     // XSPH weight c/rho0 instead of c
+    ORACLE_WALL_DENSITY = 4, // boundary faces carry the density of a fluid half-space
 };
 
 // Field ids shared with the Python wrapper (oracle/oracle.py).
@@ -121,6 +122,7 @@ template <typename T> inline V3<T> cross(const V3<T>& a, const V3<T>& b) {
 
 template <typename T> struct Consts {
     T h, h2, invH, poly6_c, spiky_c, wdq, inv_wdq, nk, rho0, rho0sq, eps, dt, jit, rmin, visc_c, vort_eps;
+    T wall_n, inv_h, wall_kd, wc3, wc5, wc7, wc9;  // wall density (see wall_term)
     int n_int;  // integer exponent of s_corr, 0 when not a small integer
 };
 
@@ -186,6 +188,17 @@ public:
             const float invPi = 0.31830988618f;
             k.poly6_c = (T)(float)(315.0f * invPi / (64.0f * std::pow(hf, 9)));
             k.spiky_c = (T)(float)(-45.0f * invPi / std::pow(hf, 6));
+        }
+        {
+            const float h2f = hf * hf, pc = (float)k.poly6_c;
+            const float h3 = (h2f * h2f) * h2f;
+            k.wall_n = (T)(p.restRho + pc * h3);
+            k.inv_h = (T)(1.0f / hf);
+            k.wall_kd = (T)(float)(315.0 / (256.0 * (double)hf));
+            k.wc3 = (T)(float)(-4.0 / 3.0);
+            k.wc5 = (T)(float)(6.0 / 5.0);
+            k.wc7 = (T)(float)(-4.0 / 7.0);
+            k.wc9 = (T)(float)(1.0 / 9.0);
         }
         V3<T> rq{(T)p.deltaq, 0, 0};
         k.wdq = W6(rq);
@@ -317,6 +330,49 @@ public:
         if (d2 >= R * R || d2 <= (T)0) return;
         const T s = R / std::sqrt(d2);
         q = {cx + d.x * s, cy + d.y * s, cz + d.z * s};
+    }
+
+    // Wall density (no reference counterpart): each boundary face is backed by a
+    // fluid half-space at rest number density wall_n; at distance d < h it adds
+    // wall_n F(d/h) to rho and wall_n dF/dd along the face normal to grad rho,
+    // F(s) = 1/2 - 315/256 (s - 4/3 s^3 + 6/5 s^5 - 4/7 s^7 + s^9/9),
+    // dF/dd = -315/(256 h) (1 - s^2)^4. Same expression sequence as the CUDA library.
+    T wall_face(T d, T& dfdd) const {
+        d = std::max(d, (T)0);
+        const T s = d * k.inv_h;
+        const T s2 = s * s;
+        T t = std::fma(s2, k.wc9, k.wc7);
+        t = std::fma(s2, t, k.wc5);
+        t = std::fma(s2, t, k.wc3);
+        t = std::fma(s2, t, (T)1);
+        const T F = (T)0.5 - (T)1.23046875 * (s * t);
+        const T om = (T)1 - s2;
+        const T om2 = om * om;
+        dfdd = -k.wall_kd * (om2 * om2);
+        return F;
+    }
+    T wall_term(const V3<T>& q, V3<T>& g) const {
+        T rho = 0;
+        const T qa[3] = {q.x, q.y, q.z};
+        T ga[3] = {0, 0, 0};
+        for (int a = 0; a < 3; ++a) {
+            const T dlo = qa[a] - (T)p.bmin[a];
+            if (dlo < k.h) {
+                T dfdd;
+                const T F = wall_face(dlo, dfdd);
+                rho = rho + k.wall_n * F;
+                ga[a] = ga[a] + k.wall_n * dfdd;
+            }
+            const T dhi = (T)p.bmax[a] - qa[a];
+            if (dhi < k.h) {
+                T dfdd;
+                const T F = wall_face(dhi, dfdd);
+                rho = rho + k.wall_n * F;
+                ga[a] = ga[a] - k.wall_n * dfdd;
+            }
+        }
+        g = {ga[0], ga[1], ga[2]};
+        return rho;
     }
 
     void dims_of(const V3<T>& q, int dim[3]) const {
@@ -453,6 +509,11 @@ public:
                     gm += dot_ref(g, g);
                 }
             }
+            if (p.flags & ORACLE_WALL_DENSITY) {
+                V3<T> gw;
+                r = r + wall_term(x[i], gw);
+                gs = {gs.x + gw.x, gs.y + gw.y, gs.z + gw.z};
+            }
             T C = r / k.rho0 - (T)1;
             if (p.flags & ORACLE_CLAMP_C) C = std::max(C, (T)0);
             if (p.arith == 1 && !is_double) {
@@ -491,6 +552,13 @@ public:
                     a = {a.x + s * g.x, a.y + s * g.y, a.z + s * g.z};
                 }
                 mag += std::fabs(s) * (std::fabs(g.x) + std::fabs(g.y) + std::fabs(g.z));
+            }
+            if (p.flags & ORACLE_WALL_DENSITY) {
+                V3<T> gw;
+                wall_term(x[i], gw);
+                a.x = std::fma(lambda[i], gw.x, a.x);
+                a.y = std::fma(lambda[i], gw.y, a.y);
+                a.z = std::fma(lambda[i], gw.z, a.z);
             }
             dp[i] = {a.x / k.rho0, a.y / k.rho0, a.z / k.rho0};
             dpmag[i] = mag / k.rho0;

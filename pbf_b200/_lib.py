@@ -21,6 +21,7 @@ PBF_ERR_NONFINITE = -6
 
 PBF_FLAG_CLAMP_C = 1
 PBF_FLAG_XSPH_RHO = 2
+PBF_FLAG_WALL_DENSITY = 4
 
 FIELD = {
     "x": 0, "v": 1, "xold": 2, "xpred": 3, "xl": 4, "rho": 5, "dp": 6, "curl": 7, "vort": 8,
@@ -51,8 +52,12 @@ class ExtParams(C.Structure):
         ("cell_order", C.c_int), ("flags", C.c_uint), ("scorr_scale", C.c_float),
         ("sphere", C.c_float * 4), ("adaptive", C.c_int), ("density_tol", C.c_float),
         ("max_iterations", C.c_int), ("measure_error", C.c_int), ("debug", C.c_int),
-        ("warm_start", C.c_int), ("reserved", C.c_int * 8),
+        ("warm_start", C.c_int), ("profile", C.c_int), ("reserved", C.c_int * 7),
     ]
+
+
+STAGES = ["hash", "scan", "scatter", "reorder", "neighbors", "lambda", "dp", "velocity", "curl", "vort", "copy",
+          "measure", "mlp"]
 
 
 class Stats(C.Structure):
@@ -83,6 +88,9 @@ _PROTOS = [
     ("pbf_field_bytes", C.c_size_t, [C.c_void_p, C.c_int]),
     ("pbf_build_grid", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pbf_get_layout", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("pbf_stage_times", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int]),
+    ("pbf_graph_kernel_count", C.c_int, [C.c_void_p]),
+    ("pbf_measure_density_error", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     ("pbf_scan_workspace_bytes", C.c_size_t, [C.c_int]),
     ("pbf_scan_exclusive_i32", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
 ]

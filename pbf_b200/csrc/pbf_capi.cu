@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/pbf.h"
 #include "pbf_kernels.h"
@@ -38,13 +39,30 @@ int fail(int code, const char* fmt, ...) {
         if (e_ != cudaSuccess) return fail(PBF_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
+// Error slots: slot k holds the density error measured after k corrections
+// (adaptive mode); slot kMaxIter + 1 holds a measurement after the loop.
+constexpr int kMaxIter = 64;
+constexpr int kSlots = kMaxIter + 2;
+
 struct DevStats {
-    unsigned long long max_bits[64];  // per iteration slot (adaptive) or slot 0
-    double sum[64];
+    unsigned long long max_bits[kSlots];
+    double sum[kSlots];
     int done;
     int iters;
+    int conv_slot;
+    int pad;
+    // not reset per substep:
     int err;
     int fallback;
+};
+
+// Profiling stages (pbf_stage_times)
+enum Stage { ST_HASH, ST_SCAN, ST_SCATTER, ST_REORDER, ST_NEIGHBORS, ST_LAMBDA, ST_DP, ST_VELOCITY, ST_CURL,
+             ST_VORT, ST_COPY, ST_MEASURE, ST_MLP, ST_COUNT };
+
+struct StageEvents {
+    int stage;
+    cudaEvent_t a, b;
 };
 
 }  // namespace
@@ -74,6 +92,8 @@ struct pbf_solver {
     cudaGraphExec_t exec = nullptr;
     cudaStream_t cap_stream = nullptr;
     cudaStream_t last_stream = nullptr;
+    std::vector<StageEvents> prof;  // event pairs captured around each launch (ext.profile)
+    int kernel_nodes = 0;
     bool uploaded = false;
     long long substeps = 0, total_iters = 0, fallbacks = 0;
 };
@@ -133,6 +153,16 @@ KParams make_kparams(const pbf_solver& s) {
     k.cell_order = e.cell_order;
     k.flags = e.flags;
     k.poly6_c64 = 315.0 / (64.0 * M_PI * std::pow((double)p.h, 9));
+    // wall density: rest number density = rho0 plus the self term W(0) that the
+    // reference's density sum leaves out
+    const float h3 = (k.h2 * k.h2) * k.h2;
+    k.wall_n = p.restRho + k.poly6_c * h3;
+    k.inv_h = 1.0f / p.h;
+    k.wall_kd = (float)(315.0 / (256.0 * (double)p.h));
+    k.wc3 = (float)(-4.0 / 3.0);
+    k.wc5 = (float)(6.0 / 5.0);
+    k.wc7 = (float)(-4.0 / 7.0);
+    k.wc9 = (float)(1.0 / 9.0);
     return k;
 }
 
@@ -153,6 +183,11 @@ void free_all(pbf_solver* s) {
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
     if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+    for (auto& e : s->prof) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    s->prof.clear();
 }
 
 int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, const pbf_ext_params* e) {
@@ -183,61 +218,87 @@ int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, co
     return PBF_OK;
 }
 
+// Wraps each launch in a pair of timing events when ext.profile is set; the
+// events are captured into the graph and read back by pbf_stage_times.
+struct Prof {
+    pbf_solver* s;
+    cudaStream_t st;
+    bool on;
+    template <typename F> void operator()(int stage, F&& f) {
+        if (!on) {
+            f();
+            return;
+        }
+        StageEvents e{stage, nullptr, nullptr};
+        cudaEventCreate(&e.a);
+        cudaEventCreate(&e.b);
+        // external record nodes: the events are recorded by every graph replay
+        cudaEventRecordWithFlags(e.a, st, cudaEventRecordExternal);
+        f();
+        cudaEventRecordWithFlags(e.b, st, cudaEventRecordExternal);
+        s->prof.push_back(e);
+    }
+};
+
 // Enqueue one substep on `st` (captured into the graph).
 void enqueue_substep(pbf_solver* s, cudaStream_t st) {
     const KParams& kp = s->kp;
     const bool dbg = s->ext.debug != 0;
     const int n = s->n;
     int* err = &s->dstats->err;
-    launch_hash(kp, true, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st);
-    if (dbg) cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
-    launch_scan(s->cnt, s->cell_start, s->ncells + 1, s->scan_ws, err, st);
-    launch_scatter(n, s->cell, s->ticket, s->cell_start, s->tmp, err, st);
-    const bool ws = s->ext.warm_start && s->mlp;
-    launch_reorder(kp, true, s->Sx, s->Sv, s->Sperm, s->cell, s->cell_start, s->tmp, s->Px, s->Pv, s->Pxold,
-                   s->Pperm, s->cell_sorted, ws ? s->lam_prev : nullptr, ws ? s->lam_prev_sorted : nullptr, err, st);
-    if (dbg) launch_copy4(n, s->Px, s->xpred_dbg, st);
-    launch_neighbors(kp, s->Px, s->cell_start, s->nbr, s->ncnt, st);
-
     DevStats* ds = s->dstats;
-    cudaMemsetAsync(ds, 0, offsetof(DevStats, err), st);  // per-substep slots, keeps err
-    const bool adaptive = s->ext.adaptive != 0;
-    int plain_iters = s->para.iterations;
-    int* skip = nullptr;
-    if (!adaptive) {
-        for (int it = 0; it < plain_iters; ++it) {
-            const bool last = it == plain_iters - 1;
-            launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, nullptr, st);
-            launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, last ? s->Pv : nullptr, s->dp_dbg, nullptr, st);
+    Prof P{s, st, s->ext.profile != 0};
+    P(ST_HASH, [&] { launch_hash(kp, true, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st); });
+    if (dbg) cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
+    P(ST_SCAN, [&] { launch_scan(s->cnt, s->cell_start, s->ncells + 1, s->scan_ws, err, st); });
+    P(ST_SCATTER, [&] { launch_scatter(n, s->cell, s->ticket, s->cell_start, s->tmp, err, st); });
+    P(ST_REORDER, [&] {
+        launch_reorder(kp, true, s->Sx, s->Sv, s->Sperm, s->cell, s->cell_start, s->tmp, s->Px, s->Pv, s->Pxold,
+                       s->Pperm, s->cell_sorted, nullptr, nullptr, err, st);
+    });
+    if (dbg) launch_copy4(n, s->Px, s->xpred_dbg, st);
+    P(ST_NEIGHBORS, [&] { launch_neighbors(kp, s->Px, s->cell_start, s->nbr, s->ncnt, st); });
+
+    cudaMemsetAsync(ds, 0, offsetof(DevStats, err), st);  // per-substep slots; keeps the error bits
+    const int iters = s->para.iterations;
+    const IterCtl fixed{};
+    if (!s->ext.adaptive) {
+        for (int it = 0; it < iters; ++it) {
+            const bool last = it == iters - 1;
+            P(ST_LAMBDA, [&] { launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, fixed, st); });
+            P(ST_DP, [&] {
+                launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, last ? s->Pv : nullptr, s->dp_dbg, fixed,
+                          st);
+            });
         }
-        if (plain_iters == 0 && ws) launch_velocity(kp, s->Px, s->Pxold, s->Pv, st);
         if (s->ext.measure_error)
-            launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[0], &ds->sum[0], nullptr, st);
+            P(ST_MEASURE, [&] {
+                launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[kSlots - 1], &ds->sum[kSlots - 1],
+                                     nullptr, st);
+            });
     } else {
-        // iterate until the max density error is within tolerance; iterations
-        // after convergence are skipped on the device (the graph is fixed)
-        const int min_it = ws ? 0 : std::max(plain_iters, 1);
+        // Iterate until the max density error is within tolerance. The graph
+        // holds max_iterations iterations; once converged the rest return at once.
+        const int min_it = std::max(iters, 1);
         const int max_it = s->ext.max_iterations;
-        if (ws) {
-            launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[0], &ds->sum[0], nullptr, st);
-            launch_check_done(&ds->max_bits[0], s->ext.density_tol, &ds->done, &ds->fallback, st);
-        }
         for (int it = 0; it < max_it; ++it) {
-            const int slot = it + 1;
-            skip = it < min_it ? nullptr : &ds->done;
-            launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, skip, st);
-            launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, nullptr, s->dp_dbg, skip, st);
-            launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[slot], &ds->sum[slot], skip, st);
-            if (it + 1 >= min_it) launch_check_done(&ds->max_bits[slot], s->ext.density_tol, &ds->done, &ds->iters, st);
-            else launch_check_done(&ds->max_bits[slot], -1.0, &ds->done, &ds->iters, st);
+            const IterCtl c{&ds->done, &ds->max_bits[it], &ds->sum[it], &ds->iters, &ds->conv_slot,
+                            (double)s->ext.density_tol, it, it >= min_it ? 1 : 0};
+            P(ST_LAMBDA, [&] { launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, c, st); });
+            P(ST_DP, [&] { launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, nullptr, s->dp_dbg, c, st); });
         }
-        launch_velocity(kp, s->Px, s->Pxold, s->Pv, st);
+        // error after the last correction, for substeps that reached the cap
+        P(ST_MEASURE, [&] {
+            launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[max_it], &ds->sum[max_it], &ds->done, st);
+        });
+        P(ST_VELOCITY, [&] { launch_velocity(kp, s->Px, s->Pxold, s->Pv, st); });
     }
-    launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, st);
-    launch_vort(kp, dbg, s->Px, s->Pv, s->omega, s->nbr, s->ncnt, s->Sv, s->Pperm, s->Sperm, s->vort_dbg,
-                s->visc_dbg, st);
-    launch_copy4(n, s->Px, s->Sx, st);
-    if (ws) cudaMemcpyAsync(s->lam_prev, s->lam0, sizeof(float) * n, cudaMemcpyDeviceToDevice, st);
+    P(ST_CURL, [&] { launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, st); });
+    P(ST_VORT, [&] {
+        launch_vort(kp, dbg, s->Px, s->Pv, s->omega, s->nbr, s->ncnt, s->Sv, s->Pperm, s->Sperm, s->vort_dbg,
+                    s->visc_dbg, st);
+    });
+    P(ST_COPY, [&] { launch_copy4(n, s->Px, s->Sx, st); });
 }
 
 int build_graph(pbf_solver* s) {
@@ -249,11 +310,26 @@ int build_graph(pbf_solver* s) {
         cudaGraphDestroy(s->graph);
         s->graph = nullptr;
     }
+    for (auto& e : s->prof) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    s->prof.clear();
     CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
     enqueue_substep(s, s->cap_stream);
     cudaError_t e = cudaStreamEndCapture(s->cap_stream, &s->graph);
     if (e != cudaSuccess) return fail(PBF_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
     CK(cudaGraphInstantiate(&s->exec, s->graph, 0));
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(s->graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CK(cudaGraphGetNodes(s->graph, nodes.data(), &nn));
+    s->kernel_nodes = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        CK(cudaGraphNodeGetType(nd, &t));
+        if (t == cudaGraphNodeTypeKernel) ++s->kernel_nodes;
+    }
     return PBF_OK;
 }
 
@@ -363,7 +439,7 @@ int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], cons
 
 int pbf_destroy(pbf_solver* s) {
     if (!s) return PBF_OK;
-    if (s->last_stream) cudaStreamSynchronize(s->last_stream);
+    cudaStreamSynchronize(s->last_stream);  // NULL is the legacy default stream
     cudaDeviceSynchronize();
     free_all(s);
     delete s;
@@ -461,7 +537,7 @@ int pbf_download(pbf_solver* s, float* pos, float* vel) {
     if (!s) return fail(PBF_ERR_INVALID, "null handle");
     if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_download before pbf_upload");
     const size_t n = s->n;
-    if (s->last_stream) CK(cudaStreamSynchronize(s->last_stream));
+    CK(cudaStreamSynchronize(s->last_stream));  // NULL is the legacy default stream
     int rc = pbf_download_device(s, s->staging, s->staging + 3 * n, nullptr);
     if (rc) return rc;
     CK(cudaStreamSynchronize(nullptr));
@@ -472,27 +548,69 @@ int pbf_download(pbf_solver* s, float* pos, float* vel) {
 
 int pbf_get_stats(pbf_solver* s, pbf_stats* out) {
     if (!s || !out) return fail(PBF_ERR_INVALID, "null argument");
-    if (s->last_stream) CK(cudaStreamSynchronize(s->last_stream));
+    CK(cudaStreamSynchronize(s->last_stream));  // NULL is the legacy default stream
     CK(cudaDeviceSynchronize());
     DevStats h;
     CK(cudaMemcpy(&h, s->dstats, sizeof h, cudaMemcpyDeviceToHost));
     std::memset(out, 0, sizeof *out);
     out->substeps = s->substeps;
     out->error_bits = h.err;
-    int slot = 0;
+    int slot = kSlots - 1;
     if (s->ext.adaptive) {
         out->last_iterations = h.iters;
-        slot = h.iters;
+        slot = h.done ? h.conv_slot : s->ext.max_iterations;
     } else {
-        out->last_iterations = s->para.iterations + ((s->ext.warm_start && s->mlp) ? 1 : 0);
+        out->last_iterations = s->para.iterations;
     }
-    if (s->ext.warm_start && s->mlp && s->ext.adaptive) out->fallbacks = h.fallback;
+    slot = std::min(std::max(slot, 0), kSlots - 1);
+    out->fallbacks = h.fallback;
     double m;
     std::memcpy(&m, &h.max_bits[slot], sizeof m);
     out->max_density_error = m;
     out->mean_density_error = h.sum[slot] / (double)s->n;
     out->total_iterations = 0;
     if (h.err) return fail(PBF_ERR_DEVICE, "kernel error bits 0x%x", h.err);
+    return PBF_OK;
+}
+
+int pbf_stage_times(pbf_solver* s, float* ms, int nstages) {
+    if (!s || !ms || nstages <= 0) return fail(PBF_ERR_INVALID, "null argument");
+    if (s->prof.empty()) return fail(PBF_ERR_STATE, "stage times need ext.profile and a pbf_step");
+    CK(cudaStreamSynchronize(s->last_stream));  // NULL is the legacy default stream
+    for (int i = 0; i < nstages; ++i) ms[i] = 0.0f;
+    for (const auto& e : s->prof) {
+        float t = 0.0f;
+        CK(cudaEventElapsedTime(&t, e.a, e.b));
+        if (e.stage < nstages) ms[e.stage] += t;
+    }
+    return PBF_OK;
+}
+
+int pbf_graph_kernel_count(pbf_solver* s) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (!s->exec) {
+        int rc = build_graph(s);
+        if (rc) return rc;
+    }
+    return s->kernel_nodes;
+}
+
+int pbf_measure_density_error(pbf_solver* s, double* max_err, double* mean_err, void* stream) {
+    if (!s || !max_err || !mean_err) return fail(PBF_ERR_INVALID, "null argument");
+    if (!s->uploaded || s->substeps == 0) return fail(PBF_ERR_STATE, "no substep has run");
+    cudaStream_t st = (cudaStream_t)stream;
+    DevStats* ds = s->dstats;
+    CK(cudaMemsetAsync(&ds->max_bits[kSlots - 1], 0, sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(&ds->sum[kSlots - 1], 0, sizeof(double), st));
+    launch_density_error(s->kp, s->Sx, s->nbr, s->ncnt, &ds->max_bits[kSlots - 1], &ds->sum[kSlots - 1], nullptr, st);
+    CK(cudaGetLastError());
+    unsigned long long mb = 0;
+    double sum = 0.0;
+    CK(cudaMemcpyAsync(&mb, &ds->max_bits[kSlots - 1], sizeof mb, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&sum, &ds->sum[kSlots - 1], sizeof sum, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::memcpy(max_err, &mb, sizeof mb);
+    *mean_err = sum / (double)s->n;
     return PBF_OK;
 }
 
@@ -538,7 +656,7 @@ int pbf_fetch(pbf_solver* s, int field, void* dst, size_t bytes) {
         default: break;
     }
     if (!src) return fail(PBF_ERR_STATE, "field %d is kept only when ext.debug is set", field);
-    if (s->last_stream) CK(cudaStreamSynchronize(s->last_stream));
+    CK(cudaStreamSynchronize(s->last_stream));  // NULL is the legacy default stream
     CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
     return PBF_OK;
 }

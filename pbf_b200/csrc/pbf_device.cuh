@@ -24,8 +24,9 @@ namespace pbf {
 
 // Flags (mirrors include/pbf.h PBF_FLAG_*)
 enum : unsigned {
-    FLAG_CLAMP_C = 1u,    // unilateral density constraint: C = max(C, 0)
-    FLAG_XSPH_RHO = 2u,   // XSPH weight c / rho0
+    FLAG_CLAMP_C = 1u,        // unilateral density constraint: C = max(C, 0)
+    FLAG_XSPH_RHO = 2u,       // XSPH weight c / rho0
+    FLAG_WALL_DENSITY = 4u,   // walls carry the density of a fluid half-space (wall_term)
 };
 
 // Error bits written by kernels into the device status word.
@@ -53,6 +54,23 @@ struct KParams {
     int n_int;      // s_corr exponent when a small integer, else 0
     unsigned flags;
     double poly6_c64;  // exact poly6 constant for the FP64 density reduction
+    // wall density: n_wall (rest number density), 1/h, 315/(256 h), Horner coefficients
+    float wall_n, inv_h, wall_kd, wc3, wc5, wc7, wc9;
+};
+
+// Device-resident control of one substep's Jacobi loop (adaptive iteration
+// counts). The lambda pass of iteration k measures the one-sided density error
+// of the positions it sees into slot k; the dp pass of iteration k ends the loop
+// when that error is within tol. done == nullptr: fixed iteration count.
+struct IterCtl {
+    int* done;
+    unsigned long long* max_bits;  // slot: max error as ordered double bits
+    double* sum;                   // slot: sum of errors
+    int* iters;                    // corrections applied
+    int* conv_slot;                // slot whose error met the tolerance
+    double tol;
+    int slot;
+    int may_stop;                  // 0 while below the minimum iteration count
 };
 
 // ---- deterministic sine ------------------------------------------------------
@@ -156,6 +174,55 @@ __device__ __forceinline__ void bound_particle(const KParams& p, f3& q) {
     if (q.z < p.bmin[2]) q.z = p.bmin[2] + p.jit * random_offset(q.x, q.y);
     if (q.z > p.bmax[2]) q.z = p.bmax[2] - p.jit * random_offset(q.x, q.y);
     if (p.sphere[3] > 0.0f) sphere_project(p, q);
+}
+
+// Wall density (no reference counterpart; stable mode). Each face of the boundary
+// box is backed by fluid at rest number density n_wall filling the half-space
+// beyond it. For a particle at distance d < h from a face, that half-space adds
+//   rho_w = n_wall F(s),  F(s) = 1/2 - (315/256) (s - 4/3 s^3 + 6/5 s^5 - 4/7 s^7 + 1/9 s^9),  s = d/h
+// (the poly6 mass beyond a plane, integrated in closed form), and its gradient
+// along the face normal, d rho_w / dd = -n_wall (315/(256 h)) (1 - s^2)^4.
+// The lambda pass adds rho_w and the gradient to rho_i and to grad_i C_i; the dp
+// pass adds lambda_i * grad rho_w / rho0.
+__device__ __forceinline__ float wall_face(const KParams& p, float d, float& dfdd) {
+    d = fmaxf(d, 0.0f);
+    const float s = d * p.inv_h;
+    const float s2 = s * s;
+    float t = __fmaf_rn(s2, p.wc9, p.wc7);
+    t = __fmaf_rn(s2, t, p.wc5);
+    t = __fmaf_rn(s2, t, p.wc3);
+    t = __fmaf_rn(s2, t, 1.0f);
+    const float F = 0.5f - 1.23046875f * (s * t);
+    const float om = 1.0f - s2;
+    const float om2 = om * om;
+    dfdd = -p.wall_kd * (om2 * om2);
+    return F;
+}
+
+__device__ __forceinline__ float wall_term(const KParams& p, const f3& q, f3& g) {
+    float rho = 0.0f;
+    g = {0.0f, 0.0f, 0.0f};
+    const float qa[3] = {q.x, q.y, q.z};
+    float ga[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float dlo = qa[a] - p.bmin[a];
+        if (dlo < p.h) {
+            float dfdd;
+            const float F = wall_face(p, dlo, dfdd);
+            rho = rho + p.wall_n * F;
+            ga[a] = ga[a] + p.wall_n * dfdd;
+        }
+        const float dhi = p.bmax[a] - qa[a];
+        if (dhi < p.h) {
+            float dfdd;
+            const float F = wall_face(p, dhi, dfdd);
+            rho = rho + p.wall_n * F;
+            ga[a] = ga[a] - p.wall_n * dfdd;
+        }
+    }
+    g = {ga[0], ga[1], ga[2]};
+    return rho;
 }
 
 // updateParticles (cu:4-13): v += dt g; x += dt v; bound

@@ -268,37 +268,70 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
 // ---------------------------------------------------------------------------
 // a9: density, constraint and lambda (calculateLambda cu:156-180)
 // ---------------------------------------------------------------------------
+// Block-wide max and sum of a per-thread error, folded into one slot with a
+// single pair of atomics per block (max as ordered double bits, value >= 0).
+__device__ __forceinline__ void block_error_reduce(float e, unsigned long long* max_bits, double* sum) {
+    __shared__ float s_max[32];
+    __shared__ float s_sum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float m = e, s = e;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    if (lane == 0) { s_max[warp] = m; s_sum[warp] = s; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double dsum = 0.0;
+        for (int w = 0; w < nw; ++w) { m = fmaxf(m, s_max[w]); dsum += (double)s_sum[w]; }
+        atomicMax(max_bits, (unsigned long long)__double_as_longlong((double)m));
+        atomicAdd(sum, dsum);
+    }
+}
+
 template <bool DEBUG>
 __global__ void __launch_bounds__(256) k_lambda(KParams p, const float4* __restrict__ x, const int* __restrict__ nbr,
                                                 const int* __restrict__ ncnt, float4* __restrict__ xl,
-                                                float* __restrict__ rho_out, const int* __restrict__ skip) {
-    if (skip && *skip) return;
+                                                float* __restrict__ rho_out, IterCtl ctl) {
+    if (ctl.done && *ctl.done) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.n) return;
-    const f3 xk = make3(x[k]);
-    const int cnt = ncnt[k];
-    float rho = 0.0f, gm = 0.0f;
-    f3 gs = {0.0f, 0.0f, 0.0f};
-    for (int q = 0; q < cnt; ++q) {
-        const int j = nbr[(size_t)q * p.stride + k];
-        const f3 r = sub3(xk, make3(x[j]));
-        const float r2 = dot_fma(r, r);
-        rho = rho + w_poly6(p, r2);
-        const f3 g = grad_spiky(p, r, r2);
-        gs = {gs.x + g.x, gs.y + g.y, gs.z + g.z};
-        gm = __fmaf_rn(g.x, g.x, gm);
-        gm = __fmaf_rn(g.y, g.y, gm);
-        gm = __fmaf_rn(g.z, g.z, gm);
+    float err = 0.0f;
+    if (k < p.n) {
+        const f3 xk = make3(x[k]);
+        const int cnt = ncnt[k];
+        float rho = 0.0f, gm = 0.0f;
+        f3 gs = {0.0f, 0.0f, 0.0f};
+        for (int q = 0; q < cnt; ++q) {
+            const int j = nbr[(size_t)q * p.stride + k];
+            const f3 r = sub3(xk, make3(x[j]));
+            const float r2 = dot_fma(r, r);
+            rho = rho + w_poly6(p, r2);
+            const f3 g = grad_spiky(p, r, r2);
+            gs = {gs.x + g.x, gs.y + g.y, gs.z + g.z};
+            gm = __fmaf_rn(g.x, g.x, gm);
+            gm = __fmaf_rn(g.y, g.y, gm);
+            gm = __fmaf_rn(g.z, g.z, gm);
+        }
+        // one-sided error of the fluid density at these positions (no wall term)
+        err = fmaxf(__fdiv_rn(rho, p.rho0) - 1.0f, 0.0f);
+        if (p.flags & FLAG_WALL_DENSITY) {
+            f3 gw;
+            rho = rho + wall_term(p, xk, gw);
+            gs = {gs.x + gw.x, gs.y + gw.y, gs.z + gw.z};
+        }
+        float C = __fdiv_rn(rho, p.rho0) - 1.0f;
+        if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
+        gm = __fmaf_rn(gs.x, gs.x, gm);
+        gm = __fmaf_rn(gs.y, gs.y, gm);
+        gm = __fmaf_rn(gs.z, gs.z, gm);
+        gm = __fdiv_rn(gm, p.rho0sq);
+        const float lam = __fdiv_rn(-C, gm + p.eps);
+        xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
+        if (DEBUG) rho_out[k] = rho;
     }
-    float C = __fdiv_rn(rho, p.rho0) - 1.0f;
-    if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
-    gm = __fmaf_rn(gs.x, gs.x, gm);
-    gm = __fmaf_rn(gs.y, gs.y, gm);
-    gm = __fmaf_rn(gs.z, gs.z, gm);
-    gm = __fdiv_rn(gm, p.rho0sq);
-    const float lam = __fdiv_rn(-C, gm + p.eps);
-    xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
-    if (DEBUG) rho_out[k] = rho;
+    if (ctl.max_bits) block_error_reduce(err, ctl.max_bits, ctl.sum);
 }
 
 // ---------------------------------------------------------------------------
@@ -310,8 +343,20 @@ template <bool DEBUG>
 __global__ void __launch_bounds__(256) k_dp(KParams p, const float4* __restrict__ xl, const int* __restrict__ nbr,
                                             const int* __restrict__ ncnt, const float4* __restrict__ xold,
                                             float4* __restrict__ xout, float4* __restrict__ vout,
-                                            float4* __restrict__ dp_out, const int* __restrict__ skip) {
-    if (skip && *skip) return;
+                                            float4* __restrict__ dp_out, IterCtl ctl) {
+    if (ctl.done) {
+        if (*ctl.done) return;
+        // the lambda pass just measured the positions this pass would correct;
+        // when they are within tolerance the loop ends here
+        if (ctl.may_stop && __longlong_as_double((long long)*ctl.max_bits) <= ctl.tol) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                *ctl.done = 1;
+                *ctl.conv_slot = ctl.slot;
+            }
+            return;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ctl.iters, 1);
+    }
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= p.n) return;
     const float4 xk4 = xl[k];
@@ -330,6 +375,13 @@ __global__ void __launch_bounds__(256) k_dp(KParams p, const float4* __restrict_
         a.x = __fmaf_rn(s, g.x, a.x);
         a.y = __fmaf_rn(s, g.y, a.y);
         a.z = __fmaf_rn(s, g.z, a.z);
+    }
+    if (p.flags & FLAG_WALL_DENSITY) {
+        f3 gw;
+        wall_term(p, xk, gw);
+        a.x = __fmaf_rn(lk, gw.x, a.x);
+        a.y = __fmaf_rn(lk, gw.y, a.y);
+        a.z = __fmaf_rn(lk, gw.z, a.z);
     }
     const f3 dp = {__fdiv_rn(a.x, p.rho0), __fdiv_rn(a.y, p.rho0), __fdiv_rn(a.z, p.rho0)};
     f3 xn = {xk.x + dp.x, xk.y + dp.y, xk.z + dp.z};
@@ -468,14 +520,6 @@ __global__ void __launch_bounds__(256) k_density_error(KParams p, const float4* 
     }
 }
 
-// Sets *done when the max error recorded so far is at or below tol.
-__global__ void k_check_done(const unsigned long long* __restrict__ max_bits, double tol, int* __restrict__ done,
-                             int* __restrict__ iters) {
-    if (*done) return;
-    *iters += 1;
-    if (__longlong_as_double((long long)*max_bits) <= tol) *done = 1;
-}
-
 // ---------------------------------------------------------------------------
 // layout kernels
 // ---------------------------------------------------------------------------
@@ -568,17 +612,17 @@ void launch_neighbors(const KParams& p, const float4* x, const int* cell_start, 
 }
 
 void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr, const int* ncnt, float4* xl,
-                   float* rho, const int* skip, cudaStream_t st) {
+                   float* rho, const IterCtl& ctl, cudaStream_t st) {
     const int b = blocks_for(p.n, 256);
-    if (debug) k_lambda<true><<<b, 256, 0, st>>>(p, x, nbr, ncnt, xl, rho, skip);
-    else k_lambda<false><<<b, 256, 0, st>>>(p, x, nbr, ncnt, xl, rho, skip);
+    if (debug) k_lambda<true><<<b, 256, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+    else k_lambda<false><<<b, 256, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
 }
 
 void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, const int* ncnt, const float4* xold,
-               float4* xout, float4* vout, float4* dp, const int* skip, cudaStream_t st) {
+               float4* xout, float4* vout, float4* dp, const IterCtl& ctl, cudaStream_t st) {
     const int b = blocks_for(p.n, 256);
-    if (debug) k_dp<true><<<b, 256, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, skip);
-    else k_dp<false><<<b, 256, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, skip);
+    if (debug) k_dp<true><<<b, 256, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+    else k_dp<false><<<b, 256, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
 }
 
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st) {
@@ -601,10 +645,6 @@ void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v,
 void launch_density_error(const KParams& p, const float4* x, const int* nbr, const int* ncnt,
                           unsigned long long* max_bits, double* sum, const int* skip, cudaStream_t st) {
     k_density_error<<<blocks_for(p.n, 256), 256, 0, st>>>(p, x, nbr, ncnt, max_bits, sum, skip);
-}
-
-void launch_check_done(const unsigned long long* max_bits, double tol, int* done, int* iters, cudaStream_t st) {
-    k_check_done<<<1, 1, 0, st>>>(max_bits, tol, done, iters);
 }
 
 void launch_from_aos(int n, const float* pos, const float* vel, float4* x, float4* v, int* perm, int* err,

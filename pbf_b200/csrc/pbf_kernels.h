@@ -20,9 +20,9 @@ void launch_reorder(const KParams& p, bool predict_on, const float4* x, const fl
                     int* perm_out, int* cell_sorted, const float* lam_in, float* lam_out, int* err, cudaStream_t st);
 void launch_neighbors(const KParams& p, const float4* x, const int* cell_start, int* nbr, int* ncnt, cudaStream_t st);
 void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr, const int* ncnt, float4* xl,
-                   float* rho, const int* skip, cudaStream_t st);
+                   float* rho, const IterCtl& ctl, cudaStream_t st);
 void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, const int* ncnt, const float4* xold,
-               float4* xout, float4* vout, float4* dp, const int* skip, cudaStream_t st);
+               float4* xout, float4* vout, float4* dp, const IterCtl& ctl, cudaStream_t st);
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st);
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
                  cudaStream_t st);
@@ -31,7 +31,6 @@ void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v,
                  cudaStream_t st);
 void launch_density_error(const KParams& p, const float4* x, const int* nbr, const int* ncnt,
                           unsigned long long* max_bits, double* sum, const int* skip, cudaStream_t st);
-void launch_check_done(const unsigned long long* max_bits, double tol, int* done, int* iters, cudaStream_t st);
 void launch_from_aos(int n, const float* pos, const float* vel, float4* x, float4* v, int* perm, int* err,
                      cudaStream_t st);
 void launch_to_aos(int n, const float4* a, const int* perm, float* out, int* err, cudaStream_t st);

@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-from ._lib import PBF_FLAG_CLAMP_C, PBF_FLAG_XSPH_RHO, ExtParams, SolverParameter
+from ._lib import PBF_FLAG_CLAMP_C, PBF_FLAG_WALL_DENSITY, PBF_FLAG_XSPH_RHO, ExtParams, SolverParameter
 from .solver import default_ext, make_parameter
 
 
@@ -60,10 +60,11 @@ def lattice_block(counts, spacing: float, origin, rng: np.random.RandomState, ji
 def stable_overrides(para: SolverParameter) -> dict:
     """Named departures for long runs (the reference formulas diverge at these
     parameters within a few substeps): unilateral density constraint, XSPH
-    weighted by 1/rho0, and s_corr expressed in lambda units, i.e. divided by
-    (sum |grad C|^2 + eps) of a rest lattice at spacing 0.5h."""
+    weighted by 1/rho0, walls that carry the density of a fluid half-space, and
+    s_corr expressed in lambda units, i.e. divided by (sum |grad C|^2 + eps) of a
+    rest lattice at spacing 0.5h."""
     g = rest_gradient_sum(float(para.h), float(para.restRho), 0.5 * float(para.h))
-    return {"flags": PBF_FLAG_CLAMP_C | PBF_FLAG_XSPH_RHO,
+    return {"flags": PBF_FLAG_CLAMP_C | PBF_FLAG_XSPH_RHO | PBF_FLAG_WALL_DENSITY,
             "scorr_scale": float(1.0 / (g + float(para.epsilon)))}
 
 

@@ -133,6 +133,25 @@ class Solver:
             check(rc)
         return {k: getattr(st, k) for k, _ in Stats._fields_}
 
+    def stage_times(self) -> dict:
+        """Per-stage milliseconds of the last substep (needs ext.profile = 1)."""
+        ms = (C.c_float * len(_lib.STAGES))()
+        check(lib().pbf_stage_times(self._h, ms, len(_lib.STAGES)))
+        return {name: float(ms[i]) for i, name in enumerate(_lib.STAGES)}
+
+    def kernel_count(self) -> int:
+        """Kernel launches per substep (kernel nodes of the substep graph)."""
+        rc = lib().pbf_graph_kernel_count(self._h)
+        if rc < 0:
+            check(rc)
+        return rc
+
+    def measure_density_error(self, stream=None):
+        """(max, mean) one-sided density error of the current state."""
+        mx, mean = C.c_double(), C.c_double()
+        check(lib().pbf_measure_density_error(self._h, C.byref(mx), C.byref(mean), _stream_handle(stream)))
+        return mx.value, mean.value
+
     def fetch(self, name: str) -> np.ndarray:
         """Internal array in cell-sorted slot order."""
         fid = _lib.FIELD[name]

@@ -1,0 +1,94 @@
+"""The C-ABI library (CPU tests: load, exports, layouts, host-side validation)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from pbf_b200 import _lib
+from pbf_b200._lib import ExtParams, SolverParameter, Stats, lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "pbf.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(pbf_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_every_declared_function_is_exported_and_bound():
+    L = lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(L, name), f"{name} declared in include/pbf.h but not exported"
+    assert set(names) <= set(_lib.declared_symbols()), set(names) - set(_lib.declared_symbols())
+
+
+def test_struct_layouts_match_the_c_side():
+    L = lib()
+    assert L.pbf_struct_size(0) == C.sizeof(SolverParameter) == 52
+    assert L.pbf_struct_size(1) == C.sizeof(ExtParams)
+    assert L.pbf_struct_size(2) == C.sizeof(Stats)
+    assert L.pbf_abi_version() == 1
+
+
+def test_defaults_are_the_reference_constants():
+    e = ExtParams()
+    lib().pbf_ext_params_default(C.byref(e))
+    assert list(e.gravity) == [0.0, -49.0, 0.0]  # kernels/cudaPBFSolver.cu:9
+    assert list(e.grid_dims) == [64, 64, 64]  # include/solverBase.h:10-12
+    assert e.max_neighbors == 63  # include/solverBase.h:6
+    assert abs(e.wall_jitter - 0.01) < 1e-9  # include/solverBase.h:5
+    assert abs(e.grad_rmin - 0.01) < 1e-9  # kernels/cudaPBFSolver.cuh:107
+    assert e.cell_scale == 1.0 and e.scorr_scale == 1.0 and e.flags == 0
+
+
+def _create(para=None, ext=None, gs=(0, 0, 0, 4, 2, 2), bd=(0.03, 0.03, 0.03, 3.97, 1.97, 1.97)):
+    from pbf_b200 import make_parameter
+    p = para or make_parameter(h=0.1, nParticles=100, restRho=6378.0, epsilon=600.0, k=0.1, n=4.0, deltaq=0.02,
+                               c=0.01, dt=1 / 120, iterations=4, vorticityConfinementEpilon=0.0005, radius=0.03)
+    e = ext or ExtParams()
+    if ext is None:
+        lib().pbf_ext_params_default(C.byref(e))
+    h = C.c_void_p()
+    rc = lib().pbf_create(C.byref(p), (C.c_float * 6)(*gs), (C.c_float * 6)(*bd), C.byref(e), C.byref(h))
+    return rc, h, p, e
+
+
+@pytest.mark.parametrize("field,value", [("nParticles", 0), ("h", 0.0), ("restRho", -1.0), ("dt", 0.0),
+                                          ("deltaq", 0.5), ("iterations", -1), ("iterations", 65),
+                                          ("epsilon", float("nan"))])
+def test_create_rejects_bad_parameters_without_touching_the_gpu(field, value):
+    rc, h, p, e = _create()
+    if rc == 0:
+        lib().pbf_destroy(h)
+    from pbf_b200 import make_parameter
+    p = make_parameter(h=0.1, nParticles=100, restRho=6378.0, epsilon=600.0, k=0.1, n=4.0, deltaq=0.02, c=0.01,
+                       dt=1 / 120, iterations=4, vorticityConfinementEpilon=0.0005, radius=0.03)
+    setattr(p, field, value)
+    rc, h, _, _ = _create(para=p)
+    assert rc == _lib.PBF_ERR_INVALID
+    assert lib().pbf_last_error()
+
+
+@pytest.mark.parametrize("field,value", [("max_neighbors", 0), ("max_neighbors", 128), ("cell_scale", 0.5),
+                                          ("cell_order", 2), ("max_iterations", 0), ("max_iterations", 65)])
+def test_create_rejects_bad_extensions(field, value):
+    e = ExtParams()
+    lib().pbf_ext_params_default(C.byref(e))
+    setattr(e, field, value)
+    rc, h, _, _ = _create(ext=e)
+    assert rc == _lib.PBF_ERR_INVALID
+
+
+def test_null_handles_are_errors_not_crashes():
+    L = lib()
+    assert L.pbf_step(None, 1, None) == _lib.PBF_ERR_INVALID
+    assert L.pbf_upload(None, None, None, 0) == _lib.PBF_ERR_INVALID
+    assert L.pbf_download(None, None, None) == _lib.PBF_ERR_INVALID
+    assert L.pbf_destroy(None) == _lib.PBF_OK
+    st = Stats()
+    assert L.pbf_get_stats(None, C.byref(st)) == _lib.PBF_ERR_INVALID
+    assert L.pbf_scan_exclusive_i32(None, None, 4, None, 0, None) == _lib.PBF_ERR_INVALID
