@@ -268,6 +268,26 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
 // ---------------------------------------------------------------------------
 // a9: density, constraint and lambda (calculateLambda cu:156-180)
 // ---------------------------------------------------------------------------
+// Neighbour gathers are issued NB at a time: NB list loads (coalesced, slot-major
+// list), then NB 16-byte position loads, so a thread keeps several memory
+// requests in flight instead of one dependent index->position chain per pair.
+constexpr int NB = 4;
+
+__device__ __forceinline__ void load_idx(const KParams& p, const int* __restrict__ nbr, int k, int q0, int cnt,
+                                         int (&jj)[NB]) {
+#pragma unroll
+    for (int u = 0; u < NB; ++u) jj[u] = (q0 + u < cnt) ? nbr[(size_t)(q0 + u) * p.stride + k] : k;
+}
+
+template <typename V>
+__device__ __forceinline__ void gather_batch(const KParams& p, const int* __restrict__ nbr, const V* __restrict__ src,
+                                             int k, int q0, int cnt, V (&out)[NB]) {
+    int jj[NB];
+    load_idx(p, nbr, k, q0, cnt, jj);
+#pragma unroll
+    for (int u = 0; u < NB; ++u) out[u] = src[jj[u]];
+}
+
 // Block-wide max and sum of a per-thread error, folded into one slot with a
 // single pair of atomics per block (max as ordered double bits, value >= 0).
 __device__ __forceinline__ void block_error_reduce(float e, unsigned long long* max_bits, double* sum) {
@@ -292,7 +312,8 @@ __device__ __forceinline__ void block_error_reduce(float e, unsigned long long* 
 }
 
 template <bool DEBUG>
-__global__ void __launch_bounds__(256) k_lambda(KParams p, const float4* __restrict__ x, const int* __restrict__ nbr,
+// 6 resident blocks per SM: 40 registers without spills (7 spills)
+__global__ void __launch_bounds__(256, 6) k_lambda(KParams p, const float4* __restrict__ x, const int* __restrict__ nbr,
                                                 const int* __restrict__ ncnt, float4* __restrict__ xl,
                                                 float* __restrict__ rho_out, IterCtl ctl) {
     if (ctl.done && *ctl.done) return;
@@ -303,16 +324,23 @@ __global__ void __launch_bounds__(256) k_lambda(KParams p, const float4* __restr
         const int cnt = ncnt[k];
         float rho = 0.0f, gm = 0.0f;
         f3 gs = {0.0f, 0.0f, 0.0f};
-        for (int q = 0; q < cnt; ++q) {
-            const int j = nbr[(size_t)q * p.stride + k];
-            const f3 r = sub3(xk, make3(x[j]));
-            const float r2 = dot_fma(r, r);
-            rho = rho + w_poly6(p, r2);
-            const f3 g = grad_spiky(p, r, r2);
-            gs = {gs.x + g.x, gs.y + g.y, gs.z + g.z};
-            gm = __fmaf_rn(g.x, g.x, gm);
-            gm = __fmaf_rn(g.y, g.y, gm);
-            gm = __fmaf_rn(g.z, g.z, gm);
+        // batches of NB neighbours: all index loads, then all position loads, then
+        // the pairs in list order (the summation order does not change)
+        for (int q0 = 0; q0 < cnt; q0 += NB) {
+            float4 xj[NB];
+            gather_batch(p, nbr, x, k, q0, cnt, xj);
+#pragma unroll
+            for (int u = 0; u < NB; ++u) {
+                if (q0 + u >= cnt) break;
+                const f3 r = sub3(xk, make3(xj[u]));
+                const float r2 = dot_fma(r, r);
+                rho = rho + w_poly6(p, r2);
+                const f3 g = grad_spiky(p, r, r2);
+                gs = {gs.x + g.x, gs.y + g.y, gs.z + g.z};
+                gm = __fmaf_rn(g.x, g.x, gm);
+                gm = __fmaf_rn(g.y, g.y, gm);
+                gm = __fmaf_rn(g.z, g.z, gm);
+            }
         }
         // one-sided error of the fluid density at these positions (no wall term)
         err = fmaxf(__fdiv_rn(rho, p.rho0) - 1.0f, 0.0f);
@@ -340,7 +368,7 @@ __global__ void __launch_bounds__(256) k_lambda(KParams p, const float4* __restr
 // (calculateOffset cu:182-199, updatePosition cu:15-22)
 // ---------------------------------------------------------------------------
 template <bool DEBUG>
-__global__ void __launch_bounds__(256) k_dp(KParams p, const float4* __restrict__ xl, const int* __restrict__ nbr,
+__global__ void __launch_bounds__(256, 6) k_dp(KParams p, const float4* __restrict__ xl, const int* __restrict__ nbr,
                                             const int* __restrict__ ncnt, const float4* __restrict__ xold,
                                             float4* __restrict__ xout, float4* __restrict__ vout,
                                             float4* __restrict__ dp_out, IterCtl ctl) {
@@ -364,17 +392,22 @@ __global__ void __launch_bounds__(256) k_dp(KParams p, const float4* __restrict_
     const float lk = xk4.w;
     const int cnt = ncnt[k];
     f3 a = {0.0f, 0.0f, 0.0f};
-    for (int q = 0; q < cnt; ++q) {
-        const int j = nbr[(size_t)q * p.stride + k];
-        const float4 xj4 = xl[j];
-        const f3 r = sub3(xk, make3(xj4));
-        const float r2 = dot_fma(r, r);
-        const float w = w_poly6(p, r2);
-        const f3 g = grad_spiky(p, r, r2);
-        const float s = (lk + xj4.w) + s_corr(p, w);
-        a.x = __fmaf_rn(s, g.x, a.x);
-        a.y = __fmaf_rn(s, g.y, a.y);
-        a.z = __fmaf_rn(s, g.z, a.z);
+    for (int q0 = 0; q0 < cnt; q0 += NB) {
+        float4 xj[NB];
+        gather_batch(p, nbr, xl, k, q0, cnt, xj);
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            if (q0 + u >= cnt) break;
+            const float4 xj4 = xj[u];
+            const f3 r = sub3(xk, make3(xj4));
+            const float r2 = dot_fma(r, r);
+            const float w = w_poly6(p, r2);
+            const f3 g = grad_spiky(p, r, r2);
+            const float s = (lk + xj4.w) + s_corr(p, w);
+            a.x = __fmaf_rn(s, g.x, a.x);
+            a.y = __fmaf_rn(s, g.y, a.y);
+            a.z = __fmaf_rn(s, g.z, a.z);
+        }
     }
     if (p.flags & FLAG_WALL_DENSITY) {
         f3 gw;
@@ -416,12 +449,23 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
     const f3 vk = make3(v[k]);
     const int cnt = ncnt[k];
     f3 w = {0.0f, 0.0f, 0.0f};
-    for (int q = 0; q < cnt; ++q) {
-        const int j = nbr[(size_t)q * p.stride + k];
-        const f3 r = sub3(xk, make3(x[j]));
-        const f3 g = grad_spiky(p, r, dot_fma(r, r));
-        const f3 c = cross3(sub3(make3(v[j]), vk), g);
-        w = {w.x + c.x, w.y + c.y, w.z + c.z};
+    for (int q0 = 0; q0 < cnt; q0 += NB) {
+        int jj[NB];
+        load_idx(p, nbr, k, q0, cnt, jj);
+        float4 xj[NB], vj[NB];
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            xj[u] = x[jj[u]];
+            vj[u] = v[jj[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            if (q0 + u >= cnt) break;
+            const f3 r = sub3(xk, make3(xj[u]));
+            const f3 g = grad_spiky(p, r, dot_fma(r, r));
+            const f3 c = cross3(sub3(make3(vj[u]), vk), g);
+            w = {w.x + c.x, w.y + c.y, w.z + c.z};
+        }
     }
     omega[k] = make_float4(w.x, w.y, w.z, 0.0f);
 }
@@ -442,21 +486,33 @@ __global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restric
     const f3 vk = make3(v[k]);
     const int cnt = ncnt[k];
     f3 pv = {0.0f, 0.0f, 0.0f}, eta = {0.0f, 0.0f, 0.0f};
-    for (int q = 0; q < cnt; ++q) {
-        const int j = nbr[(size_t)q * p.stride + k];
-        const f3 r = sub3(xk, make3(x[j]));
-        const float r2 = dot_fma(r, r);
-        const float w = w_poly6(p, r2);
-        const f3 vji = sub3(make3(v[j]), vk);
-        pv.x = __fmaf_rn(vji.x, w, pv.x);
-        pv.y = __fmaf_rn(vji.y, w, pv.y);
-        pv.z = __fmaf_rn(vji.z, w, pv.z);
-        const f3 oj = make3(omega[j]);
-        const float wl = __fsqrt_rn(dot_fma(oj, oj));
-        const f3 g = grad_spiky(p, r, r2);
-        eta.x = __fmaf_rn(wl, g.x, eta.x);
-        eta.y = __fmaf_rn(wl, g.y, eta.y);
-        eta.z = __fmaf_rn(wl, g.z, eta.z);
+    for (int q0 = 0; q0 < cnt; q0 += NB) {
+        int jj[NB];
+        load_idx(p, nbr, k, q0, cnt, jj);
+        float4 xj[NB], vj[NB], oj4[NB];
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            xj[u] = x[jj[u]];
+            vj[u] = v[jj[u]];
+            oj4[u] = omega[jj[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            if (q0 + u >= cnt) break;
+            const f3 r = sub3(xk, make3(xj[u]));
+            const float r2 = dot_fma(r, r);
+            const float w = w_poly6(p, r2);
+            const f3 vji = sub3(make3(vj[u]), vk);
+            pv.x = __fmaf_rn(vji.x, w, pv.x);
+            pv.y = __fmaf_rn(vji.y, w, pv.y);
+            pv.z = __fmaf_rn(vji.z, w, pv.z);
+            const f3 oj = make3(oj4[u]);
+            const float wl = __fsqrt_rn(dot_fma(oj, oj));
+            const f3 g = grad_spiky(p, r, r2);
+            eta.x = __fmaf_rn(wl, g.x, eta.x);
+            eta.y = __fmaf_rn(wl, g.y, eta.y);
+            eta.z = __fmaf_rn(wl, g.z, eta.z);
+        }
     }
     const float el = __fsqrt_rn(dot_fma(eta, eta));
     if ((double)el > 1e-3) eta = {__fdiv_rn(eta.x, el), __fdiv_rn(eta.y, el), __fdiv_rn(eta.z, el)};
