@@ -66,7 +66,8 @@ typedef struct pbf_solver_parameter {
 typedef struct pbf_ext_params {
     float gravity[3];    /* default (0,-49,0): kernels/cudaPBFSolver.cu:9 */
     int grid_dims[3];    /* default 64^3: include/solverBase.h:10-12 */
-    float cell_scale;    /* cell edge = h * cell_scale, >= 1 (default 1) */
+    float cell_scale;    /* cell edge = h * cell_scale, >= 0.25 (default 1); below 1 the
+                            stencil reaches ceil(1 / cell_scale) cells each way */
     float wall_jitter;   /* wall offset coefficient (default 0.01, RANDOM_OFFSET_COEFF) */
     float grad_rmin;     /* spiky gradient lower cutoff (default 0.01, cuh:107) */
     int max_neighbors;   /* neighbour cap, 1..127 (default 63, MAX_NEIGHBOR) */
@@ -124,6 +125,29 @@ void pbf_ext_params_default(pbf_ext_params* ext);
  * wall the particles are clamped to. */
 int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], const float boundary[6],
                const pbf_ext_params* ext, pbf_solver** out);
+
+/* One scene of a batch (no reference counterpart): its grid anchor and wall
+ * box, grid cells per axis, particle count and sphere obstacle. */
+typedef struct pbf_scene_desc {
+    float grid_space[6];
+    float boundary[6];
+    int grid_dims[3];
+    int nparticles;
+    float sphere[4];  /* centre xyz, radius (<= 0: none) */
+} pbf_scene_desc;
+
+/* Many independent scenes advanced together: every phase of a substep is one
+ * launch over all scenes' particles, and one scan over the concatenated cell
+ * keys of all scenes sorts every scene at once. para->nParticles must be the
+ * sum of the scenes' counts; positions and velocities are uploaded and
+ * downloaded concatenated in scene order. ext->grid_dims and ext->sphere are
+ * taken from the scene descriptions instead. */
+int pbf_create_batch(const pbf_solver_parameter* para, int nscenes, const pbf_scene_desc* scenes,
+                     const pbf_ext_params* ext, pbf_solver** out);
+
+/* Layout of scene `scene`: first cell key, real cells, first particle slot,
+ * particle count. */
+int pbf_get_scene_layout(const pbf_solver* s, int scene, int* cell_base, int* ncells, int* pbase, int* pcount);
 
 /* Replaces freeCUDASolverDataBuffer (kernels/cudaPBF.cu:32-48). */
 int pbf_destroy(pbf_solver* s);

@@ -462,15 +462,20 @@ public:
             int d[3];
             dims_of(x[i], d);
             if (p.formulation == 0) {
-                for (int j = 0; j < 27 && c < cap; ++j) {
-                    int nd[3] = {d[0] + j % 3 - 1, d[1] + (j / 3) % 3 - 1, d[2] + j / 9 - 1};
-                    const int g = gid(nd);
-                    if (g < 0) continue;
-                    for (int s = start[g]; s < end[g] && c < cap; ++s) {
-                        const int jj = sorted[s];
-                        if (jj != i) append(i, jj, c);
-                    }
-                }
+                // dz-major, dy, dx fastest (j % 3, j / 3 % 3, j / 9 for R = 1); cells
+                // smaller than h widen the stencil to R = ceil(1 / cell_scale)
+                const int R = p.cell_scale >= 1.0f ? 1 : (int)std::ceil(1.0 / (double)p.cell_scale);
+                for (int dz = -R; dz <= R && c < cap; ++dz)
+                    for (int dy = -R; dy <= R && c < cap; ++dy)
+                        for (int dx = -R; dx <= R && c < cap; ++dx) {
+                            int nd[3] = {d[0] + dx, d[1] + dy, d[2] + dz};
+                            const int g = gid(nd);
+                            if (g < 0) continue;
+                            for (int s = start[g]; s < end[g] && c < cap; ++s) {
+                                const int jj = sorted[s];
+                                if (jj != i) append(i, jj, c);
+                            }
+                        }
             } else {
                 for (int ox = -1; ox <= 1 && c < cap; ++ox)
                     for (int oy = -1; oy <= 1 && c < cap; ++oy)

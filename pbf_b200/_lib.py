@@ -60,6 +60,15 @@ STAGES = ["hash", "scan", "scatter", "reorder", "neighbors", "lambda", "dp", "ve
           "measure", "mlp"]
 
 
+class SceneDesc(C.Structure):
+    """pbf_scene_desc (include/pbf.h)."""
+
+    _fields_ = [
+        ("grid_space", C.c_float * 6), ("boundary", C.c_float * 6), ("grid_dims", C.c_int * 3),
+        ("nparticles", C.c_int), ("sphere", C.c_float * 4),
+    ]
+
+
 class Stats(C.Structure):
     _fields_ = [
         ("substeps", C.c_longlong), ("total_iterations", C.c_longlong), ("fallbacks", C.c_longlong),
@@ -76,6 +85,10 @@ _PROTOS = [
     ("pbf_ext_params_default", None, [C.POINTER(ExtParams)]),
     ("pbf_create", C.c_int, [C.POINTER(SolverParameter), C.POINTER(C.c_float), C.POINTER(C.c_float),
                              C.POINTER(ExtParams), C.POINTER(C.c_void_p)]),
+    ("pbf_create_batch", C.c_int, [C.POINTER(SolverParameter), C.c_int, C.POINTER(SceneDesc),
+                                   C.POINTER(ExtParams), C.POINTER(C.c_void_p)]),
+    ("pbf_get_scene_layout", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("pbf_destroy", C.c_int, [C.c_void_p]),
     ("pbf_upload", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     ("pbf_upload_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),

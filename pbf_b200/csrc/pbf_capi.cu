@@ -72,7 +72,10 @@ struct pbf_solver {
     pbf_ext_params ext{};
     float grid_space[6]{}, boundary[6]{};
     KParams kp{};
-    int n = 0, ncells = 0, stride = 0;
+    int n = 0, ncells = 0, nkeys = 0, stride = 0;  // ncells: real cells of scene 0
+    std::vector<SceneView> scenes_h;
+    SceneView* scenes_d = nullptr;  // scene table (batches)
+    int* sid = nullptr;             // per slot: scene index (batches)
     // device state (slot order)
     float4 *Sx = nullptr, *Sv = nullptr, *Px = nullptr, *Pv = nullptr, *Pxold = nullptr, *Q = nullptr,
            *omega = nullptr;
@@ -138,16 +141,14 @@ KParams make_kparams(const pbf_solver& s) {
     k.rmin = e.grad_rmin;
     k.visc_c = (e.flags & PBF_FLAG_XSPH_RHO) ? (float)((double)p.c / (double)p.restRho) : p.c;
     k.vort_eps = p.vorticityConfinementEpilon;
-    for (int a = 0; a < 3; ++a) {
-        k.g[a] = e.gravity[a];
-        k.gmin[a] = s.grid_space[a];
-        k.bmin[a] = s.boundary[a];
-        k.bmax[a] = s.boundary[3 + a];
-        k.dims[a] = e.grid_dims[a];
-    }
-    for (int a = 0; a < 4; ++a) k.sphere[a] = e.sphere[a];
+    for (int a = 0; a < 3; ++a) k.g[a] = e.gravity[a];
+    k.sc0 = s.scenes_h[0];
+    k.scenes = s.scenes_d;
+    k.sid = s.sid;
+    k.nscenes = (int)s.scenes_h.size();
+    k.nkeys = s.nkeys;
+    k.radius = e.cell_scale >= 1.0f ? 1 : (int)std::ceil(1.0 / (double)e.cell_scale);
     k.n = s.n;
-    k.ncells = s.ncells;
     k.max_nbr = e.max_neighbors;
     k.stride = s.stride;
     k.cell_order = e.cell_order;
@@ -177,7 +178,7 @@ void free_all(pbf_solver* s) {
     void* ptrs[] = {s->Sx, s->Sv, s->Px, s->Pv, s->Pxold, s->Q, s->omega, s->xpred_dbg, s->dp_dbg, s->vort_dbg,
                     s->visc_dbg, s->rho_dbg, s->Sperm, s->Pperm, s->cell, s->ticket, s->tmp, s->cell_sorted,
                     s->ncnt, s->nbr, s->cnt, s->cell_start, s->hash_dbg, s->lam_prev, s->lam_prev_sorted, s->lam0,
-                    s->scan_ws, s->dstats, s->staging};
+                    s->scan_ws, s->dstats, s->staging, s->scenes_d, s->sid};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->exec) cudaGraphExecDestroy(s->exec);
@@ -188,6 +189,21 @@ void free_all(pbf_solver* s) {
         cudaEventDestroy(e.b);
     }
     s->prof.clear();
+}
+
+int validate_scene(const pbf_scene_desc& d, int idx) {
+    if (!finite6(d.grid_space) || !finite6(d.boundary))
+        return fail(PBF_ERR_INVALID, "scene %d: non-finite grid space or boundary", idx);
+    for (int a = 0; a < 3; ++a) {
+        if (d.grid_dims[a] <= 0) return fail(PBF_ERR_INVALID, "scene %d: grid_dims must be positive", idx);
+        if (d.boundary[a] > d.boundary[3 + a]) return fail(PBF_ERR_INVALID, "scene %d: boundary pMin > pMax", idx);
+    }
+    for (int a = 0; a < 4; ++a)
+        if (!std::isfinite(d.sphere[a])) return fail(PBF_ERR_INVALID, "scene %d: non-finite sphere", idx);
+    const long long cells = (long long)d.grid_dims[0] * d.grid_dims[1] * d.grid_dims[2];
+    if (cells > (1ll << 30)) return fail(PBF_ERR_INVALID, "scene %d: grid has too many cells (%lld)", idx, cells);
+    if (d.nparticles <= 0) return fail(PBF_ERR_INVALID, "scene %d: nparticles must be positive", idx);
+    return PBF_OK;
 }
 
 int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, const pbf_ext_params* e) {
@@ -208,7 +224,8 @@ int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, co
     }
     const long long cells = (long long)e->grid_dims[0] * e->grid_dims[1] * e->grid_dims[2];
     if (cells > (1ll << 30)) return fail(PBF_ERR_INVALID, "grid has too many cells (%lld)", cells);
-    if (!(e->cell_scale >= 1.0f) || !std::isfinite(e->cell_scale)) return fail(PBF_ERR_INVALID, "cell_scale must be >= 1");
+    if (!(e->cell_scale >= 0.25f) || !std::isfinite(e->cell_scale))
+        return fail(PBF_ERR_INVALID, "cell_scale must be >= 0.25");
     if (e->max_neighbors < 1 || e->max_neighbors > 127) return fail(PBF_ERR_INVALID, "max_neighbors must lie in [1, 127]");
     if (e->cell_order != 0 && e->cell_order != 1) return fail(PBF_ERR_INVALID, "cell_order must be 0 or 1");
     if (e->max_iterations < 1 || e->max_iterations > 64) return fail(PBF_ERR_INVALID, "max_iterations must lie in [1, 64]");
@@ -250,7 +267,7 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
     Prof P{s, st, s->ext.profile != 0};
     P(ST_HASH, [&] { launch_hash(kp, true, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st); });
     if (dbg) cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
-    P(ST_SCAN, [&] { launch_scan(s->cnt, s->cell_start, s->ncells + 1, s->scan_ws, err, st); });
+    P(ST_SCAN, [&] { launch_scan(s->cnt, s->cell_start, s->nkeys, s->scan_ws, err, st); });
     P(ST_SCATTER, [&] { launch_scatter(n, s->cell, s->ticket, s->cell_start, s->tmp, err, st); });
     P(ST_REORDER, [&] {
         launch_reorder(kp, true, s->Sx, s->Sv, s->Sperm, s->cell, s->cell_start, s->tmp, s->Px, s->Pv, s->Pxold,
@@ -333,6 +350,10 @@ int build_graph(pbf_solver* s) {
     return PBF_OK;
 }
 
+// Allocates a solver over `nscenes` validated scene descriptions (defined below).
+int create_common(const pbf_solver_parameter* para, int nscenes, const pbf_scene_desc* descs,
+                  const pbf_ext_params* ext, pbf_solver** out);
+
 }  // namespace
 
 extern "C" {
@@ -379,14 +400,90 @@ int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], cons
     }
     int rc = validate(para, grid_space, boundary, ext);
     if (rc) return rc;
+    pbf_scene_desc d{};
+    std::memcpy(d.grid_space, grid_space, sizeof d.grid_space);
+    std::memcpy(d.boundary, boundary, sizeof d.boundary);
+    for (int a = 0; a < 3; ++a) d.grid_dims[a] = ext->grid_dims[a];
+    for (int a = 0; a < 4; ++a) d.sphere[a] = ext->sphere[a];
+    d.nparticles = para->nParticles;
+    return create_common(para, 1, &d, ext, out);
+}
+
+int pbf_create_batch(const pbf_solver_parameter* para, int nscenes, const pbf_scene_desc* scenes,
+                     const pbf_ext_params* ext, pbf_solver** out) {
+    if (!out) return fail(PBF_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    if (!para || !scenes || nscenes <= 0) return fail(PBF_ERR_INVALID, "need a parameter block and >= 1 scene");
+    pbf_ext_params def;
+    if (!ext) {
+        pbf_ext_params_default(&def);
+        ext = &def;
+    }
+    long long total = 0;
+    for (int i = 0; i < nscenes; ++i) {
+        int rc = validate_scene(scenes[i], i);
+        if (rc) return rc;
+        total += scenes[i].nparticles;
+    }
+    if (total != para->nParticles)
+        return fail(PBF_ERR_INVALID, "nParticles (%d) differs from the scenes' total (%lld)", para->nParticles, total);
+    int rc = validate(para, scenes[0].grid_space, scenes[0].boundary, ext);
+    if (rc) return rc;
+    return create_common(para, nscenes, scenes, ext, out);
+}
+
+int pbf_get_scene_layout(const pbf_solver* s, int scene, int* cell_base, int* ncells, int* pbase, int* pcount) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (scene < 0 || scene >= (int)s->scenes_h.size()) return fail(PBF_ERR_INVALID, "scene %d out of range", scene);
+    const SceneView& v = s->scenes_h[scene];
+    if (cell_base) *cell_base = v.cell_base;
+    if (ncells) *ncells = v.ncells;
+    if (pbase) *pbase = v.pbase;
+    if (pcount) *pcount = v.pcount;
+    return PBF_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int create_common(const pbf_solver_parameter* para, int nscenes, const pbf_scene_desc* descs,
+                  const pbf_ext_params* ext, pbf_solver** out) {
+    int rc = PBF_OK;
     pbf_solver* s = new (std::nothrow) pbf_solver();
     if (!s) return fail(PBF_ERR_ALLOC, "host allocation failed");
     s->para = *para;
     s->ext = *ext;
-    std::memcpy(s->grid_space, grid_space, sizeof s->grid_space);
-    std::memcpy(s->boundary, boundary, sizeof s->boundary);
+    std::memcpy(s->grid_space, descs[0].grid_space, sizeof s->grid_space);
+    std::memcpy(s->boundary, descs[0].boundary, sizeof s->boundary);
     s->n = para->nParticles;
-    s->ncells = ext->grid_dims[0] * ext->grid_dims[1] * ext->grid_dims[2];
+    // scene table: keys of scene i are [cell_base, cell_base + ncells], the last
+    // being its out-of-grid bin; its particles occupy slots [pbase, pbase + pcount)
+    long long keys = 0, slots = 0;
+    for (int i = 0; i < nscenes; ++i) {
+        const pbf_scene_desc& d = descs[i];
+        SceneView v{};
+        for (int a = 0; a < 3; ++a) {
+            v.gmin[a] = d.grid_space[a];
+            v.bmin[a] = d.boundary[a];
+            v.bmax[a] = d.boundary[3 + a];
+            v.dims[a] = d.grid_dims[a];
+        }
+        for (int a = 0; a < 4; ++a) v.sphere[a] = d.sphere[a];
+        v.ncells = d.grid_dims[0] * d.grid_dims[1] * d.grid_dims[2];
+        v.cell_base = (int)keys;
+        v.pbase = (int)slots;
+        v.pcount = d.nparticles;
+        keys += (long long)v.ncells + 1;
+        slots += d.nparticles;
+        s->scenes_h.push_back(v);
+    }
+    if (keys >= (1ll << 31) - 1) {
+        delete s;
+        return fail(PBF_ERR_INVALID, "too many cells over all scenes (%lld)", keys);
+    }
+    s->nkeys = (int)keys;
+    s->ncells = s->scenes_h[0].ncells;
     s->stride = (s->n + 31) & ~31;
     const size_t n = s->n;
     const bool dbg = ext->debug != 0;
@@ -403,8 +500,8 @@ int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], cons
     AL(s->Sperm, n); AL(s->Pperm, n); AL(s->cell, n); AL(s->ticket, n); AL(s->tmp, n); AL(s->cell_sorted, n);
     AL(s->ncnt, n);
     AL(s->nbr, (size_t)ext->max_neighbors * s->stride);
-    AL(s->cnt, (size_t)s->ncells + 1);
-    AL(s->cell_start, (size_t)s->ncells + 2);
+    AL(s->cnt, (size_t)s->nkeys);
+    AL(s->cell_start, (size_t)s->nkeys + 1);
     AL(s->lam_prev, n); AL(s->lam_prev_sorted, n); AL(s->lam0, n);
     AL(s->staging, 6 * n);
     AL(s->dstats, 1);
@@ -412,8 +509,12 @@ int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], cons
         AL(s->xpred_dbg, n); AL(s->dp_dbg, n); AL(s->vort_dbg, n); AL(s->visc_dbg, n); AL(s->rho_dbg, n);
         AL(s->hash_dbg, n);
     }
+    if (nscenes > 1) {
+        AL(s->scenes_d, (size_t)nscenes);
+        AL(s->sid, n);
+    }
     {
-        const size_t ws = scan_status_bytes(s->ncells + 1);
+        const size_t ws = scan_status_bytes(s->nkeys);
         cudaError_t e = cudaMalloc(&s->scan_ws, ws);
         if (e != cudaSuccess) {
             free_all(s);
@@ -422,7 +523,14 @@ int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], cons
         }
     }
 #undef AL
-    cudaError_t e = cudaMemset(s->cnt, 0, sizeof(int) * (s->ncells + 1));
+    cudaError_t e = cudaMemset(s->cnt, 0, sizeof(int) * (size_t)s->nkeys);
+    if (e == cudaSuccess && nscenes > 1) {
+        e = cudaMemcpy(s->scenes_d, s->scenes_h.data(), sizeof(SceneView) * nscenes, cudaMemcpyHostToDevice);
+        std::vector<int> sid(n);
+        for (int i = 0; i < nscenes; ++i)
+            for (int k = 0; k < s->scenes_h[i].pcount; ++k) sid[s->scenes_h[i].pbase + k] = i;
+        if (e == cudaSuccess) e = cudaMemcpy(s->sid, sid.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemset(s->dstats, 0, sizeof(DevStats));
     if (e == cudaSuccess) e = cudaMemset(s->lam_prev, 0, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaMemset(s->lam0, 0, sizeof(float) * n);
@@ -436,6 +544,10 @@ int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], cons
     *out = s;
     return PBF_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int pbf_destroy(pbf_solver* s) {
     if (!s) return PBF_OK;
@@ -508,7 +620,7 @@ int pbf_build_grid(pbf_solver* s, void* stream) {
     int* err = &s->dstats->err;
     launch_hash(kp, false, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st);
     if (s->hash_dbg) CK(cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * s->n, cudaMemcpyDeviceToDevice, st));
-    launch_scan(s->cnt, s->cell_start, s->ncells + 1, s->scan_ws, err, st);
+    launch_scan(s->cnt, s->cell_start, s->nkeys, s->scan_ws, err, st);
     launch_scatter(s->n, s->cell, s->ticket, s->cell_start, s->tmp, err, st);
     launch_reorder(kp, false, s->Sx, s->Sv, s->Sperm, s->cell, s->cell_start, s->tmp, s->Px, s->Pv, s->Pxold, s->Pperm,
                    s->cell_sorted, nullptr, nullptr, err, st);
@@ -623,7 +735,7 @@ size_t pbf_field_bytes(const pbf_solver* s, int field) {
             return n * sizeof(float4);
         case PBF_FIELD_RHO: case PBF_FIELD_LAMBDA0: return n * sizeof(float);
         case PBF_FIELD_CELL: case PBF_FIELD_PERM: case PBF_FIELD_NCNT: case PBF_FIELD_HASH: return n * sizeof(int);
-        case PBF_FIELD_CELL_START: return ((size_t)s->ncells + 2) * sizeof(int);
+        case PBF_FIELD_CELL_START: return ((size_t)s->nkeys + 1) * sizeof(int);
         case PBF_FIELD_NBR: return (size_t)s->ext.max_neighbors * s->stride * sizeof(int);
         default: return 0;
     }

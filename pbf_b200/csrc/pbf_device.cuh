@@ -37,17 +37,33 @@ enum : int {
     DEVERR_MLP_TIMEOUT = 8,     // tensor-core pipeline gave up waiting on an mbarrier
 };
 
+// One scene of a batch: its uniform grid, wall box and obstacle, and where its
+// cell keys and particle slots lie in the batch-wide arrays. Keys of scene s are
+// cell_base .. cell_base + ncells, the last one being the scene's out-of-grid
+// bin, so a single scan over all keys keeps every scene's particles contiguous.
+struct SceneView {
+    float gmin[3];
+    float bmin[3], bmax[3];
+    float sphere[4];
+    int dims[3];
+    int cell_base;  // first key of the scene
+    int ncells;     // real cells; key cell_base + ncells is the out-of-grid bin
+    int pbase;      // first particle slot of the scene
+    int pcount;
+};
+
 struct KParams {
     // kernel constants, all computed on the host (pbf_capi.cu: make_kparams)
     float h, h2, inv_cell, poly6_c, spiky_c, inv_wdq, nk, scorr_scale, n_exp;
     float rho0, rho0sq, eps, dt, jit, rmin, visc_c, vort_eps;
     float g[3];
-    float gmin[3];
-    float bmin[3], bmax[3];
-    float sphere[4];
-    int dims[3];
+    SceneView sc0;              // the scene when there is one
+    const SceneView* scenes;    // device table when nscenes > 1
+    const int* sid;             // per slot: scene index (slots never leave their scene)
+    int nscenes;
+    int nkeys;      // cell keys over all scenes (cells + one out-of-grid bin per scene)
+    int radius;     // stencil radius in cells: ceil(1 / cell_scale)
     int n;          // particles
-    int ncells;     // real cells; slot ncells is the out-of-grid bin
     int max_nbr;    // neighbour cap (reference MAX_NEIGHBOR = 63)
     int stride;     // neighbour list stride (slot-major layout: nbr[q * stride + k])
     int cell_order; // 0 ascending, 1 descending within a cell
@@ -156,24 +172,30 @@ __device__ __forceinline__ float random_offset(float u, float v) {
 
 // Static sphere obstacle (no reference counterpart): a point inside the sphere is
 // moved radially onto its surface.
-__device__ __forceinline__ void sphere_project(const KParams& p, f3& q) {
-    const float R = p.sphere[3];
-    const f3 d = {q.x - p.sphere[0], q.y - p.sphere[1], q.z - p.sphere[2]};
+__device__ __forceinline__ void sphere_project(const SceneView& sc, f3& q) {
+    const float R = sc.sphere[3];
+    const f3 d = {q.x - sc.sphere[0], q.y - sc.sphere[1], q.z - sc.sphere[2]};
     const float d2 = dot_fma(d, d);
     if (d2 >= R * R || d2 <= 0.0f) return;
     const float s = __fdiv_rn(R, __fsqrt_rn(d2));
-    q = {p.sphere[0] + d.x * s, p.sphere[1] + d.y * s, p.sphere[2] + d.z * s};
+    q = {sc.sphere[0] + d.x * s, sc.sphere[1] + d.y * s, sc.sphere[2] + d.z * s};
+}
+
+// The scene of slot k (slots never leave their scene's range).
+__device__ __forceinline__ SceneView scene_of(const KParams& p, int k) {
+    if (p.nscenes == 1) return p.sc0;
+    return p.scenes[p.sid[k]];
 }
 
 // BoundParticle (cuh:121-140), including the reference's y-max branch that hashes (y, z)
-__device__ __forceinline__ void bound_particle(const KParams& p, f3& q) {
-    if (q.x < p.bmin[0]) q.x = p.bmin[0] + p.jit * random_offset(q.y, q.z);
-    if (q.x > p.bmax[0]) q.x = p.bmax[0] - p.jit * random_offset(q.y, q.z);
-    if (q.y < p.bmin[1]) q.y = p.bmin[1] + p.jit * random_offset(q.x, q.z);
-    if (q.y > p.bmax[1]) q.y = p.bmax[1] - p.jit * random_offset(q.y, q.z);
-    if (q.z < p.bmin[2]) q.z = p.bmin[2] + p.jit * random_offset(q.x, q.y);
-    if (q.z > p.bmax[2]) q.z = p.bmax[2] - p.jit * random_offset(q.x, q.y);
-    if (p.sphere[3] > 0.0f) sphere_project(p, q);
+__device__ __forceinline__ void bound_particle(const KParams& p, const SceneView& sc, f3& q) {
+    if (q.x < sc.bmin[0]) q.x = sc.bmin[0] + p.jit * random_offset(q.y, q.z);
+    if (q.x > sc.bmax[0]) q.x = sc.bmax[0] - p.jit * random_offset(q.y, q.z);
+    if (q.y < sc.bmin[1]) q.y = sc.bmin[1] + p.jit * random_offset(q.x, q.z);
+    if (q.y > sc.bmax[1]) q.y = sc.bmax[1] - p.jit * random_offset(q.y, q.z);
+    if (q.z < sc.bmin[2]) q.z = sc.bmin[2] + p.jit * random_offset(q.x, q.y);
+    if (q.z > sc.bmax[2]) q.z = sc.bmax[2] - p.jit * random_offset(q.x, q.y);
+    if (sc.sphere[3] > 0.0f) sphere_project(sc, q);
 }
 
 // Wall density (no reference counterpart; stable mode). Each face of the boundary
@@ -199,21 +221,21 @@ __device__ __forceinline__ float wall_face(const KParams& p, float d, float& dfd
     return F;
 }
 
-__device__ __forceinline__ float wall_term(const KParams& p, const f3& q, f3& g) {
+__device__ __forceinline__ float wall_term(const KParams& p, const SceneView& sc, const f3& q, f3& g) {
     float rho = 0.0f;
     g = {0.0f, 0.0f, 0.0f};
     const float qa[3] = {q.x, q.y, q.z};
     float ga[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float dlo = qa[a] - p.bmin[a];
+        const float dlo = qa[a] - sc.bmin[a];
         if (dlo < p.h) {
             float dfdd;
             const float F = wall_face(p, dlo, dfdd);
             rho = rho + p.wall_n * F;
             ga[a] = ga[a] + p.wall_n * dfdd;
         }
-        const float dhi = p.bmax[a] - qa[a];
+        const float dhi = sc.bmax[a] - qa[a];
         if (dhi < p.h) {
             float dfdd;
             const float F = wall_face(p, dhi, dfdd);
@@ -226,26 +248,27 @@ __device__ __forceinline__ float wall_term(const KParams& p, const f3& q, f3& g)
 }
 
 // updateParticles (cu:4-13): v += dt g; x += dt v; bound
-__device__ __forceinline__ void predict(const KParams& p, f3& x, f3& v) {
+__device__ __forceinline__ void predict(const KParams& p, const SceneView& sc, f3& x, f3& v) {
     v = {v.x + p.dt * p.g[0], v.y + p.dt * p.g[1], v.z + p.dt * p.g[2]};
     x = {x.x + p.dt * v.x, x.y + p.dt * v.y, x.z + p.dt * v.z};
-    bound_particle(p, x);
+    bound_particle(p, sc, x);
 }
 
 // computeDimID (cuh:156-160): truncation toward zero
-__device__ __forceinline__ void cell_dims(const KParams& p, const f3& x, int d[3]) {
-    d[0] = (int)((x.x - p.gmin[0]) * p.inv_cell);
-    d[1] = (int)((x.y - p.gmin[1]) * p.inv_cell);
-    d[2] = (int)((x.z - p.gmin[2]) * p.inv_cell);
+__device__ __forceinline__ void cell_dims(const KParams& p, const SceneView& sc, const f3& x, int d[3]) {
+    d[0] = (int)((x.x - sc.gmin[0]) * p.inv_cell);
+    d[1] = (int)((x.y - sc.gmin[1]) * p.inv_cell);
+    d[2] = (int)((x.z - sc.gmin[2]) * p.inv_cell);
 }
 
-// computeGid (cuh:172-181) with the out-of-grid particles mapped to bin ncells
-__device__ __forceinline__ int cell_key(const KParams& p, const f3& x) {
+// computeGid (cuh:172-181) offset by the scene's first key; out-of-grid particles
+// go to the scene's out-of-grid bin
+__device__ __forceinline__ int cell_key(const KParams& p, const SceneView& sc, const f3& x) {
     int d[3];
-    cell_dims(p, x, d);
-    if (d[0] < 0 || d[0] >= p.dims[0] || d[1] < 0 || d[1] >= p.dims[1] || d[2] < 0 || d[2] >= p.dims[2])
-        return p.ncells;
-    return d[0] + d[1] * p.dims[0] + d[2] * p.dims[0] * p.dims[1];
+    cell_dims(p, sc, x, d);
+    if (d[0] < 0 || d[0] >= sc.dims[0] || d[1] < 0 || d[1] >= sc.dims[1] || d[2] < 0 || d[2] >= sc.dims[2])
+        return sc.cell_base + sc.ncells;
+    return sc.cell_base + d[0] + d[1] * sc.dims[0] + d[2] * sc.dims[0] * sc.dims[1];
 }
 
 }  // namespace pbf

@@ -31,13 +31,14 @@ __global__ void __launch_bounds__(256) k_hash(KParams p, const float4* __restric
     const int lane = threadIdx.x & 31;
     int key = -1;
     if (i < p.n) {
+        const SceneView sc = scene_of(p, i);
         f3 xi = make3(x[i]);
         if (PREDICT) {
             f3 vi = make3(v[i]);
-            predict(p, xi, vi);
+            predict(p, sc, xi, vi);
         }
         if (!(isfinite(xi.x) && isfinite(xi.y) && isfinite(xi.z))) atomicOr(err, DEVERR_NONFINITE);
-        key = cell_key(p, xi);
+        key = cell_key(p, sc, xi);
     }
     // warp-aggregated histogram: one atomic per distinct cell in the warp
     const unsigned peers = __match_any_sync(0xffffffffu, key);
@@ -205,7 +206,8 @@ __global__ void __launch_bounds__(256) k_reorder(KParams p, const float4* __rest
         atomicOr(err, DEVERR_BAD_INDEX);
         return;
     }
-    const bool desc = p.cell_order == 1 && c < p.ncells;
+    const SceneView sc = scene_of(p, i);
+    const bool desc = p.cell_order == 1 && c != sc.cell_base + sc.ncells;  // out-of-grid bin stays ascending
     int q = 0;
     for (int k = s; k < e; ++k) {
         const int o = tmp[k];
@@ -215,7 +217,7 @@ __global__ void __launch_bounds__(256) k_reorder(KParams p, const float4* __rest
     const float4 x4 = x[i];
     f3 xi = make3(x4);
     f3 vi = make3(v[i]);
-    if (PREDICT) predict(p, xi, vi);
+    if (PREDICT) predict(p, sc, xi, vi);
     xp[dst] = make_float4(xi.x, xi.y, xi.z, 0.0f);
     vp[dst] = make_float4(vi.x, vi.y, vi.z, 0.0f);
     xold[dst] = make_float4(x4.x, x4.y, x4.z, 0.0f);
@@ -225,31 +227,34 @@ __global__ void __launch_bounds__(256) k_reorder(KParams p, const float4* __rest
 }
 
 // ---------------------------------------------------------------------------
-// a7: 27-cell neighbour search. The stencil is visited dz-major, dy, then the
-// three dx cells of a row, which are one contiguous slot range because keys are
-// x-fastest; within a cell, slot order. This is the reference order
-// (buildNeighborhood cu:133-136) applied to the sorted slots.
+// a7: 27-cell neighbour search (a (2R+1)^3 stencil when cells are smaller than
+// h). The stencil is visited dz-major, dy, then the dx cells of a row, which are
+// one contiguous slot range because keys are x-fastest; within a cell, slot
+// order. For R = 1 this is the reference order (buildNeighborhood cu:133-136)
+// applied to the sorted slots.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __restrict__ x,
                                                    const int* __restrict__ cell_start, int* __restrict__ nbr,
                                                    int* __restrict__ ncnt) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= p.n) return;
+    const SceneView sc = scene_of(p, k);
     const f3 xk = make3(x[k]);
     int d[3];
-    cell_dims(p, xk, d);
-    const int nx = p.dims[0], ny = p.dims[1], nz = p.dims[2];
-    const int x0 = max(d[0] - 1, 0), x1 = min(d[0] + 1, nx - 1);
+    cell_dims(p, sc, xk, d);
+    const int nx = sc.dims[0], ny = sc.dims[1], nz = sc.dims[2];
+    const int R = p.radius;
+    const int x0 = max(d[0] - R, 0), x1 = min(d[0] + R, nx - 1);
     int c = 0;
     const int cap = p.max_nbr;
     if (x0 <= x1) {
-        for (int dz = -1; dz <= 1 && c < cap; ++dz) {
+        for (int dz = -R; dz <= R && c < cap; ++dz) {
             const int z = d[2] + dz;
             if (z < 0 || z >= nz) continue;
-            for (int dy = -1; dy <= 1 && c < cap; ++dy) {
+            for (int dy = -R; dy <= R && c < cap; ++dy) {
                 const int y = d[1] + dy;
                 if (y < 0 || y >= ny) continue;
-                const int row = y * nx + z * nx * ny;
+                const int row = sc.cell_base + y * nx + z * nx * ny;
                 const int s = cell_start[row + x0], e = cell_start[row + x1 + 1];
                 for (int j = s; j < e && c < cap; ++j) {
                     if (j == k) continue;
@@ -346,7 +351,7 @@ __global__ void __launch_bounds__(256, 6) k_lambda(KParams p, const float4* __re
         err = fmaxf(__fdiv_rn(rho, p.rho0) - 1.0f, 0.0f);
         if (p.flags & FLAG_WALL_DENSITY) {
             f3 gw;
-            rho = rho + wall_term(p, xk, gw);
+            rho = rho + wall_term(p, scene_of(p, k), xk, gw);
             gs = {gs.x + gw.x, gs.y + gw.y, gs.z + gw.z};
         }
         float C = __fdiv_rn(rho, p.rho0) - 1.0f;
@@ -411,14 +416,14 @@ __global__ void __launch_bounds__(256, 6) k_dp(KParams p, const float4* __restri
     }
     if (p.flags & FLAG_WALL_DENSITY) {
         f3 gw;
-        wall_term(p, xk, gw);
+        wall_term(p, scene_of(p, k), xk, gw);
         a.x = __fmaf_rn(lk, gw.x, a.x);
         a.y = __fmaf_rn(lk, gw.y, a.y);
         a.z = __fmaf_rn(lk, gw.z, a.z);
     }
     const f3 dp = {__fdiv_rn(a.x, p.rho0), __fdiv_rn(a.y, p.rho0), __fdiv_rn(a.z, p.rho0)};
     f3 xn = {xk.x + dp.x, xk.y + dp.y, xk.z + dp.z};
-    bound_particle(p, xn);
+    bound_particle(p, scene_of(p, k), xn);
     xout[k] = make_float4(xn.x, xn.y, xn.z, 0.0f);
     if (vout) {
         const float4 xo = xold[k];

@@ -167,3 +167,81 @@ def reference_app_scene(idx: int, seed: int = 0, dims=(64, 64, 64)) -> Scene:
     ov = {"gravity": (0.0, -49.0, 0.0), "grid_dims": [64, 64, 64]}
     return Scene(f"reference_app_scene_{idx}", para, box, bd, ov, pos.astype(np.float32), vel.astype(np.float32),
                  info={"scene": idx, "seed": seed})
+
+
+# ---- batches of independent scenes --------------------------------------------
+def random_block_scene(n: int, rng: np.random.RandomState, h: float = 0.1, iterations: int = 4,
+                       stable: bool = True, jitter: float = 0.01) -> Scene:
+    """n particles in a cube-ish jittered lattice block (x-fastest, spacing 0.5h)
+    at a random position on the floor of a box twice the block's size, stretched
+    in x by an aspect ratio drawn from U[1, 3]."""
+    spacing = 0.5 * h
+    m = max(2, int(round(n ** (1.0 / 3.0))))
+    counts = (m, m, int(np.ceil(n / (m * m))))
+    extent = [c * spacing for c in counts]
+    side = 2.0 * max(extent) + 4 * spacing
+    aspect = rng.uniform(1.0, 3.0)
+    cells = (int(np.ceil(side * aspect / h)), int(np.ceil(side / h)), int(np.ceil(side / h)))
+    box = [0.0, 0.0, 0.0, cells[0] * h, cells[1] * h, cells[2] * h]
+    origin = (rng.uniform(spacing, box[3] - extent[0] - spacing), spacing + rng.uniform(0.0, 0.25 * box[4]),
+              rng.uniform(spacing, box[5] - extent[2] - spacing))
+    pos = lattice_block(counts, spacing, origin, rng, jitter * h)[:n]
+    vel = np.zeros_like(pos)
+    para = benchmark_parameter(n, h=h, iterations=iterations)
+    r = float(para.radius)
+    bd = [box[0] + r, box[1] + r, box[2] + r, box[3] - r, box[4] - r, box[5] - r]
+    ov = {"gravity": (0.0, -9.8, 0.0), "grid_dims": list(cells)}
+    if stable:
+        ov.update(stable_overrides(para))
+    return Scene(f"block_{n}", para, box, bd, ov, pos, vel, info={"aspect": aspect, "counts": counts})
+
+
+def config2(seed: int = 0, n_scenes: int = 64, lo: int = 4096, hi: int = 65536, iterations: int = 4,
+            stable: bool = True) -> list:
+    """64 scenes with particle counts log-uniform in [4,096, 65,536] (seeded)."""
+    rng = np.random.RandomState(seed)
+    counts = np.exp(rng.uniform(np.log(lo), np.log(hi), size=n_scenes)).round().astype(int)
+    return [random_block_scene(int(c), rng, iterations=iterations, stable=stable) for c in counts]
+
+
+def config4(seed: int = 0, block: int = 128, iterations: int = 4, stable: bool = True, small: int = 65536,
+            n_small: int = 8) -> list:
+    """Double dam break: two block^3 jittered lattices facing each other in a
+    320h x 160h x 160h box with a static sphere of radius 20h at the centre,
+    batched with n_small scenes of `small` particles."""
+    h = 0.1
+    spacing = 0.5 * h
+    rng = np.random.RandomState(seed)
+    cells = (320, 160, 160)
+    box = [0.0, 0.0, 0.0, cells[0] * h, cells[1] * h, cells[2] * h]
+    ext = block * spacing
+    zc = 0.5 * (box[5] - ext)
+    a = lattice_block((block, block, block), spacing, (spacing, spacing, zc), rng, 0.01 * h)
+    b = lattice_block((block, block, block), spacing, (box[3] - ext, spacing, zc), rng, 0.01 * h)
+    pos = np.concatenate([a, b])
+    n = pos.shape[0]
+    para = benchmark_parameter(n, h=h, iterations=iterations)
+    r = float(para.radius)
+    bd = [box[0] + r, box[1] + r, box[2] + r, box[3] - r, box[4] - r, box[5] - r]
+    sphere = (0.5 * box[3], 20 * h, 0.5 * box[5], 20 * h)
+    ov = {"gravity": (0.0, -9.8, 0.0), "grid_dims": list(cells), "sphere": sphere}
+    if stable:
+        ov.update(stable_overrides(para))
+    big = Scene(f"double_dam_break_{n}", para, box, bd, ov, pos, np.zeros_like(pos), info={"sphere": sphere})
+    return [big] + [random_block_scene(small, rng, iterations=iterations, stable=stable) for _ in range(n_small)]
+
+
+def batch_inputs(scenes: list, iterations: Optional[int] = None):
+    """(SolverParameter, scene descriptions, ext overrides, positions, velocities)
+    for a BatchSolver over `scenes`; they share parameters and flags."""
+    total = sum(s.n for s in scenes)
+    p0 = scenes[0].para
+    para = benchmark_parameter(total, h=float(p0.h), iterations=int(p0.iterations if iterations is None else iterations))
+    descs = []
+    for s in scenes:
+        descs.append({"grid_space": s.grid_space, "boundary": s.boundary, "grid_dims": s.ext_overrides["grid_dims"],
+                      "nparticles": s.n, "sphere": s.ext_overrides.get("sphere", (0.0, 0.0, 0.0, 0.0))})
+    ov = {k: v for k, v in scenes[0].ext_overrides.items() if k not in ("grid_dims", "sphere")}
+    pos = np.concatenate([s.pos for s in scenes])
+    vel = np.concatenate([s.vel for s in scenes])
+    return para, descs, ov, pos, vel

@@ -181,6 +181,41 @@ class Solver:
         return [nbr[: cnt[k], k].tolist() for k in range(self.n)]
 
 
+class BatchSolver(Solver):
+    """Many independent scenes in one handle (pbf_create_batch): every phase of
+    a substep is one launch over all scenes; positions and velocities are
+    concatenated in scene order. All scenes share the SolverParameter values and
+    the ext flags; each has its own grid, wall box and obstacle."""
+
+    def __init__(self, para: SolverParameter, scenes: Sequence[dict], ext: Optional[ExtParams] = None):
+        """scenes: dicts with grid_space, boundary, grid_dims, nparticles, optional sphere."""
+        self.para = para
+        self.ext = ext if ext is not None else default_ext()
+        self.n = int(para.nParticles)
+        descs = (_lib.SceneDesc * len(scenes))()
+        for i, d in enumerate(scenes):
+            for a in range(6):
+                descs[i].grid_space[a] = float(d["grid_space"][a])
+                descs[i].boundary[a] = float(d["boundary"][a])
+            for a in range(3):
+                descs[i].grid_dims[a] = int(d["grid_dims"][a])
+            descs[i].nparticles = int(d["nparticles"])
+            for a, v in enumerate(d.get("sphere", (0.0, 0.0, 0.0, 0.0))):
+                descs[i].sphere[a] = float(v)
+        h = C.c_void_p()
+        check(lib().pbf_create_batch(C.byref(para), len(scenes), descs, C.byref(self.ext), C.byref(h)))
+        self._h = h
+        nc, st, mn = C.c_int(), C.c_int(), C.c_int()
+        check(lib().pbf_get_layout(h, C.byref(nc), C.byref(st), C.byref(mn)))
+        self.ncells, self.stride, self.max_neighbors = nc.value, st.value, mn.value
+        self.nscenes = len(scenes)
+
+    def scene_layout(self, i: int) -> dict:
+        cb, nc, pb, pc = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().pbf_get_scene_layout(self._h, i, C.byref(cb), C.byref(nc), C.byref(pb), C.byref(pc)))
+        return {"cell_base": cb.value, "ncells": nc.value, "pbase": pb.value, "pcount": pc.value}
+
+
 class PBFSolver:
     """The reference CPU solver's interface (include/solver.h:86-111) on the GPU
     step: construct with the parameters and box, then solve(particles) advances

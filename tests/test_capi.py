@@ -73,7 +73,7 @@ def test_create_rejects_bad_parameters_without_touching_the_gpu(field, value):
     assert lib().pbf_last_error()
 
 
-@pytest.mark.parametrize("field,value", [("max_neighbors", 0), ("max_neighbors", 128), ("cell_scale", 0.5),
+@pytest.mark.parametrize("field,value", [("max_neighbors", 0), ("max_neighbors", 128), ("cell_scale", 0.2),
                                           ("cell_order", 2), ("max_iterations", 0), ("max_iterations", 65)])
 def test_create_rejects_bad_extensions(field, value):
     e = ExtParams()
