@@ -208,10 +208,14 @@ def run_b200(args) -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    from pbf_b200 import autotune
     sc = scenes.config1(seed=rank, iterations=4)
     n = sc.n
     stream = torch.cuda.current_stream()
-    solver = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(profile=1))
+    tuned = autotune.tune([sc], iterations=4)
+    ext_kw = dict(grid_dims=autotune.dims_for_scale(sc.ext_overrides["grid_dims"], tuned["cell_scale"]),
+                  cell_scale=tuned["cell_scale"], block_size=tuned["block_size"])
+    solver = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(**ext_kw))
     solver.upload(sc.pos, sc.vel)
     kernels = solver.kernel_count()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
@@ -219,30 +223,42 @@ def run_b200(args) -> int:
     for _ in range(max(args.warmup, 3)):
         solver.step(1, stream)
     torch.cuda.synchronize()
+    state_pos, state_vel = solver.download()  # start of the timed region, reused by the profiled pass
 
-    stage_acc = {}
     errs = []
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        time.sleep(0.3)  # let the sampler start before the timed steps
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record(stream)
             solver.step(1, stream)
             ev[k][1].record(stream)
-            torch.cuda.synchronize()
-            for name, ms in solver.stage_times().items():
-                stage_acc[name] = stage_acc.get(name, 0.0) + ms
-            errs.append(solver.measure_density_error(stream))
+            errs.append(solver.measure_density_error(stream))  # after the step's end event
         torch.cuda.synchronize()
+        time.sleep(0.3)
     barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     tot_s = max_over_ranks(sum(step_ms) / 1e3)
     value = n * world * args.steps / tot_s
-    stages = {k: v / args.steps for k, v in stage_acc.items() if v > 0}
     ncnt = solver.fetch("ncnt")
     pairs = float(ncnt.sum())
+
+    # Per-kernel durations: the same K substeps from the same state on a handle
+    # whose graph records a CUDA event pair around every launch (the event nodes
+    # slow the graph down, so the headline timing above runs without them).
+    prof = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(profile=1, **ext_kw))
+    prof.upload(state_pos, state_vel)
+    stage_acc = {}
+    for k in range(args.steps):
+        flush.zero_()
+        prof.step(1, stream)
+        for name, ms in prof.stage_times().items():
+            stage_acc[name] = stage_acc.get(name, 0.0) + ms
+    stages = {k: v / args.steps for k, v in stage_acc.items() if v > 0}
+    prof.close()
 
     # L2-warm throughput: the same substeps back to back without flushing
     warm = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -306,11 +322,14 @@ def run_b200(args) -> int:
         "roofline_step": {"alg_bytes_per_step": step_bytes, "achieved_gbs": step_bytes / (tot_s / args.steps) / 1e9,
                           "frac_hbm": step_bytes / (tot_s / args.steps) / 1e9 / hbm_peak},
         "stages_ms": {k: round(v, 5) for k, v in stages.items()},
+        "stages_note": "per-kernel CUDA-event times from a profiled pass over the same K substeps and state",
+        "autotune": {"cell_scale": tuned["cell_scale"], "block_size": tuned["block_size"], "table": tuned["table"]},
         "value_l2_warm": n * world * args.steps / warm_s,
         "density_error": {"max": max(e[0] for e in errs), "mean": statistics.mean(e[1] for e in errs),
                           "target_max": 0.01, "meets_target": max(e[0] for e in errs) <= 0.01},
         "clocks": clocks,
     }
+    out["batched"] = measure_batched(args, rank, world, dev, flush, stream, barrier, max_over_ranks)
     if rank == 0 and world == 1:
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0:
@@ -319,6 +338,48 @@ def run_b200(args) -> int:
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def measure_batched(args, rank, world, dev, flush, stream, barrier, max_over_ranks) -> dict:
+    """64 independent scenes (particle counts log-uniform in [4,096, 65,536],
+    seeded), one launch per phase over all scenes of this rank, block size and
+    cell size chosen by the autotuner; scenes are sharded over ranks."""
+    import torch
+
+    from pbf_b200 import BatchSolver, autotune, multigpu, scenes
+    scs = scenes.config2(seed=0)
+    parts = multigpu.assign_scenes([s.n for s in scs], world)
+    mine = [scs[i] for i in parts[rank]]
+    tuned = autotune.tune(mine, iterations=4)
+    para, descs, ov, pos, vel = scenes.batch_inputs(mine, iterations=4)
+    for d in descs:
+        d["grid_dims"] = autotune.dims_for_scale(d["grid_dims"], tuned["cell_scale"])
+    ov.update(cell_scale=tuned["cell_scale"], block_size=tuned["block_size"])
+    b = BatchSolver(para, descs, scenes.default_ext(**ov))
+    b.upload(pos, vel)
+    b.step(max(args.warmup, 3), stream)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    errs = []
+    barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        b.step(1, stream)
+        ev[k][1].record(stream)
+        errs.append(b.measure_density_error(stream))
+    torch.cuda.synchronize()
+    barrier()
+    t = max_over_ranks(sum(a.elapsed_time(c) for a, c in ev) / 1e3)
+    total = sum(s.n for s in scs)
+    out = {"workload": "64 scenes, counts log-uniform in [4096, 65536] (seed 0), box aspect U[1,3], 4 iterations",
+           "scenes": len(scs), "particles": total, "value": total * args.steps / t, "unit": UNIT,
+           "ms_per_step": 1e3 * t / args.steps, "kernels_per_step": b.kernel_count(),
+           "autotune": {"cell_scale": tuned["cell_scale"], "block_size": tuned["block_size"],
+                        "table": tuned["table"]},
+           "density_error": {"max": max(e[0] for e in errs), "mean": statistics.mean(e[1] for e in errs)}}
+    b.close()
+    return out
 
 
 def load_traffic(kernel: str):

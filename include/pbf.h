@@ -82,7 +82,8 @@ typedef struct pbf_ext_params {
     int debug;           /* 1: keep per-stage intermediates for pbf_fetch */
     int warm_start;      /* 1: learned lambda warm start (needs installed weights) */
     int profile;         /* 1: time every launch with CUDA events (pbf_stage_times) */
-    int reserved[7];
+    int block_size;      /* threads per block of the neighbour passes: 0 (= 256), 64, 128 or 256 */
+    int reserved[6];
 } pbf_ext_params;
 
 typedef struct pbf_stats {

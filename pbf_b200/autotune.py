@@ -1,0 +1,84 @@
+"""Autotuner for the neighbour passes: picks the threads per block and the grid
+cell size (h or h/2 with a 5x5x5 stencil) of a workload by timing each
+candidate on the GPU from the same initial state, and caches the choice.
+
+The candidates change only the launch shape and the neighbour-list order, not
+the neighbour sets (test_gpu_batch.py checks the sets for cells of h/2).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+from typing import Optional, Sequence
+
+CANDIDATES = [(cs, bs) for cs in (1.0, 0.5) for bs in (128, 256)]
+
+
+def dims_for_scale(dims: Sequence[int], cell_scale: float) -> list:
+    """Grid cells per axis covering the same extent with cells of h * cell_scale."""
+    return [int(math.ceil(d / cell_scale - 1e-9)) for d in dims]
+
+
+def signature(scenes, iterations: int) -> str:
+    n = sum(s.n for s in scenes)
+    return f"scenes={len(scenes)}:n={n}:h={float(scenes[0].para.h):.6g}:it={iterations}"
+
+
+def _time_candidate(scenes, iterations, cell_scale, block, substeps, warm):
+    import torch
+
+    from . import scenes as S
+    from .solver import BatchSolver, Solver
+    scs = list(scenes)
+    if len(scs) == 1:
+        sc = scs[0]
+        dims = dims_for_scale(sc.ext_overrides["grid_dims"], cell_scale)
+        s = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(grid_dims=dims, cell_scale=cell_scale, block_size=block))
+        s.upload(sc.pos, sc.vel)
+    else:
+        para, descs, ov, pos, vel = S.batch_inputs(scs, iterations=iterations)
+        for d in descs:
+            d["grid_dims"] = dims_for_scale(d["grid_dims"], cell_scale)
+        ov.update(cell_scale=cell_scale, block_size=block)
+        s = BatchSolver(para, descs, S.default_ext(**ov))
+        s.upload(pos, vel)
+    st = torch.cuda.current_stream()
+    s.step(warm, st)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    s.step(substeps, st)
+    b.record(st)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / substeps
+    s.close()
+    return ms
+
+
+def tune(scenes, iterations: int = 4, substeps: int = 6, warm: int = 2, candidates=None,
+         cache_path: Optional[str] = None) -> dict:
+    """Times every (cell_scale, block_size) candidate and returns the fastest:
+    {"cell_scale", "block_size", "ms_per_substep", "table"}."""
+    key = signature(scenes, iterations)
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+        if key in cache:
+            return cache[key]
+    table = []
+    for cs, bs in candidates or CANDIDATES:
+        table.append({"cell_scale": cs, "block_size": bs,
+                      "ms_per_substep": _time_candidate(scenes, iterations, cs, bs, substeps, warm)})
+    best = min(table, key=lambda r: r["ms_per_substep"])
+    out = dict(best)
+    out["table"] = table
+    if cache_path:
+        cache = {}
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                cache = json.load(f)
+        cache[key] = out
+        os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1)
+    return out

@@ -149,6 +149,7 @@ KParams make_kparams(const pbf_solver& s) {
     k.nkeys = s.nkeys;
     k.radius = e.cell_scale >= 1.0f ? 1 : (int)std::ceil(1.0 / (double)e.cell_scale);
     k.n = s.n;
+    k.block = e.block_size > 0 ? e.block_size : 256;
     k.max_nbr = e.max_neighbors;
     k.stride = s.stride;
     k.cell_order = e.cell_order;
@@ -228,6 +229,8 @@ int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, co
         return fail(PBF_ERR_INVALID, "cell_scale must be >= 0.25");
     if (e->max_neighbors < 1 || e->max_neighbors > 127) return fail(PBF_ERR_INVALID, "max_neighbors must lie in [1, 127]");
     if (e->cell_order != 0 && e->cell_order != 1) return fail(PBF_ERR_INVALID, "cell_order must be 0 or 1");
+    if (e->block_size != 0 && e->block_size != 64 && e->block_size != 128 && e->block_size != 256)
+        return fail(PBF_ERR_INVALID, "block_size must be 0, 64, 128 or 256");
     if (e->max_iterations < 1 || e->max_iterations > 64) return fail(PBF_ERR_INVALID, "max_iterations must lie in [1, 64]");
     if (e->adaptive && p->iterations > e->max_iterations)
         return fail(PBF_ERR_INVALID, "iterations exceeds max_iterations");

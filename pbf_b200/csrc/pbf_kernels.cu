@@ -669,21 +669,21 @@ void launch_reorder(const KParams& p, bool predict_on, const float4* x, const fl
 }
 
 void launch_neighbors(const KParams& p, const float4* x, const int* cell_start, int* nbr, int* ncnt, cudaStream_t st) {
-    k_neighbors<<<blocks_for(p.n, 256), 256, 0, st>>>(p, x, cell_start, nbr, ncnt);
+    k_neighbors<<<blocks_for(p.n, p.block), p.block, 0, st>>>(p, x, cell_start, nbr, ncnt);
 }
 
 void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr, const int* ncnt, float4* xl,
                    float* rho, const IterCtl& ctl, cudaStream_t st) {
-    const int b = blocks_for(p.n, 256);
-    if (debug) k_lambda<true><<<b, 256, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
-    else k_lambda<false><<<b, 256, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+    const int b = blocks_for(p.n, p.block);
+    if (debug) k_lambda<true><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+    else k_lambda<false><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
 }
 
 void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, const int* ncnt, const float4* xold,
                float4* xout, float4* vout, float4* dp, const IterCtl& ctl, cudaStream_t st) {
-    const int b = blocks_for(p.n, 256);
-    if (debug) k_dp<true><<<b, 256, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
-    else k_dp<false><<<b, 256, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+    const int b = blocks_for(p.n, p.block);
+    if (debug) k_dp<true><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+    else k_dp<false><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
 }
 
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st) {
@@ -692,15 +692,15 @@ void launch_velocity(const KParams& p, const float4* x, const float4* xold, floa
 
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
                  cudaStream_t st) {
-    k_curl<<<blocks_for(p.n, 256), 256, 0, st>>>(p, x, v, nbr, ncnt, omega);
+    k_curl<<<blocks_for(p.n, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, omega);
 }
 
 void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v, const float4* omega, const int* nbr,
                  const int* ncnt, float4* vout, const int* perm_in, int* perm_out, float4* vort, float4* visc,
                  cudaStream_t st) {
-    const int b = blocks_for(p.n, 256);
-    if (debug) k_vort<true><<<b, 256, 0, st>>>(p, x, v, omega, nbr, ncnt, vout, perm_in, perm_out, vort, visc);
-    else k_vort<false><<<b, 256, 0, st>>>(p, x, v, omega, nbr, ncnt, vout, perm_in, perm_out, vort, visc);
+    const int b = blocks_for(p.n, p.block);
+    if (debug) k_vort<true><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, vout, perm_in, perm_out, vort, visc);
+    else k_vort<false><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, vout, perm_in, perm_out, vort, visc);
 }
 
 void launch_density_error(const KParams& p, const float4* x, const int* nbr, const int* ncnt,
