@@ -92,3 +92,31 @@ def test_null_handles_are_errors_not_crashes():
     st = Stats()
     assert L.pbf_get_stats(None, C.byref(st)) == _lib.PBF_ERR_INVALID
     assert L.pbf_scan_exclusive_i32(None, None, 4, None, 0, None) == _lib.PBF_ERR_INVALID
+
+
+REF = os.environ.get("PBF_REFERENCE_DIR", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "include")), reason="reference headers not present")
+def test_reference_shim_exports_the_reference_symbols(tmp_path):
+    """reference_shim.cpp compiles against the reference's own headers and
+    defines the same (mangled) functions the reference's kernels/cudaPBF.cu does."""
+    import subprocess
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    obj = tmp_path / "shim.o"
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    subprocess.run([cxx, "-std=c++17", "-c", f"-I{REF}/include", f"-I{REF}/ext", f"-I{REF}/ext/glfw/include",
+                    f"-I{repo}/include", os.path.join(repo, "pbf_b200", "csrc", "reference_shim.cpp"), "-o",
+                    str(obj)], check=True)
+    ours = subprocess.run(["nm", "-g", "--defined-only", str(obj)], capture_output=True, text=True).stdout
+    want = ["cudaPBFSolve", "initCUDASolverDataBuffer", "freeCUDASolverDataBuffer"]
+    ref_so = os.path.join(repo, "oracle", "_ref", "libpbfref_gpu.so")
+    if os.path.exists(ref_so):
+        theirs = subprocess.run(["nm", "-D", "--defined-only", ref_so], capture_output=True, text=True).stdout
+        for name in want:
+            ms = {l.split()[-1] for l in theirs.splitlines() if name in l}
+            mo = {l.split()[-1] for l in ours.splitlines() if name in l}
+            assert ms and ms == mo, (name, ms, mo)
+    else:
+        for name in want:
+            assert name in ours
