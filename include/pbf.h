@@ -83,7 +83,8 @@ typedef struct pbf_ext_params {
     int warm_start;      /* 1: learned lambda warm start (needs installed weights) */
     int profile;         /* 1: time every launch with CUDA events (pbf_stage_times) */
     int block_size;      /* threads per block of the neighbour passes: 0 (= 256), 64, 128 or 256 */
-    int reserved[6];
+    int record_features; /* 1: keep warm-start features and total lambda (training data) */
+    int reserved[5];
 } pbf_ext_params;
 
 typedef struct pbf_stats {
@@ -116,6 +117,8 @@ typedef struct pbf_solver pbf_solver;
 #define PBF_FIELD_NBR 14       /* int[max_neighbors * stride] slot-major neighbour slots */
 #define PBF_FIELD_HASH 15      /* int[n] cell key per particle before sorting (debug) */
 #define PBF_FIELD_LAMBDA0 16   /* float[n] warm-start lambda of the last substep */
+#define PBF_FIELD_FEATURES 17  /* float[n * 12] warm-start features of the last substep */
+#define PBF_FIELD_LAMBDA_TOTAL 18 /* float[n] total lambda applied in the last substep */
 
 void pbf_ext_params_default(pbf_ext_params* ext);
 
@@ -214,6 +217,49 @@ int pbf_measure_density_error(pbf_solver* s, double* max_err, double* mean_err, 
  * The input is left unchanged. */
 size_t pbf_scan_workspace_bytes(int n);
 int pbf_scan_exclusive_i32(const int* d_in, int* d_out, int n, void* d_ws, size_t ws_bytes, void* stream);
+
+/* ---- Learned lambda warm start (no reference counterpart) --------------------
+ * A per-particle MLP, 12 features -> 64 -> 64 -> 64 -> 1 with GELU, BF16
+ * weights and FP32 accumulation on the tensor cores, predicts the substep's
+ * total lambda from the features of the first lambda pass; that prediction is
+ * applied as the first correction, then the plain Jacobi iterations follow (and,
+ * with ext.adaptive, continue while the density error exceeds ext.density_tol).
+ * Weights: W1[64][16], W2[64][64], W3[64][64], w4[64] row-major [out][in]
+ * (9,280 values); constants: b1[64], b2[64], b3[64], b4, feature mean[16],
+ * feature 1/std[16], output scale (226 floats). */
+#define PBF_MLP_NUM_WEIGHTS 9280
+#define PBF_MLP_NUM_BIASES 226
+
+/* Installs warm-start weights (BF16 bit patterns) and constants in a solver. */
+int pbf_set_warm_start(pbf_solver* s, const unsigned short* w_bf16, size_t n_w, const float* b_f32, size_t n_b);
+
+/* Training rows from the last substep (ext.record_features): for each slot in
+ * d_slots, its 12 features to d_feat[i * 12] and its total lambda to d_target[i]. */
+int pbf_gather_training_rows(pbf_solver* s, const int* d_slots, int count, float* d_feat, float* d_target,
+                             void* stream);
+
+/* Trainer: FP32 master weights, Adam state, and tensor-core forward/backward
+ * kernels; loss = mean (output - target / output scale)^2. */
+typedef struct pbf_mlp_trainer pbf_mlp_trainer;
+int pbf_mlp_trainer_create(int max_batch, const float* w32, const float* b32, pbf_mlp_trainer** out);
+int pbf_mlp_trainer_destroy(pbf_mlp_trainer* t);
+/* Gradients of the loss over a batch (device features [batch][12], targets
+ * [batch]); copies them (9,280 + 226 floats, zeros for the constants) and the
+ * loss to host memory when the pointers are not null. */
+int pbf_mlp_gradients(pbf_mlp_trainer* t, const float* d_feat, const float* d_target, int batch, float* h_gw,
+                      float* h_gb, float* h_loss, void* stream);
+/* Gradients plus one Adam step (beta 0.9 / 0.999, eps 1e-8). */
+int pbf_mlp_train_step(pbf_mlp_trainer* t, const float* d_feat, const float* d_target, int batch, float lr,
+                       float* h_loss, void* stream);
+int pbf_mlp_get_params(pbf_mlp_trainer* t, float* w32, float* b32, unsigned short* w_bf16);
+/* lambda0 for a batch of feature rows with the trainer's current weights. */
+int pbf_mlp_forward(pbf_mlp_trainer* t, const float* d_feat, int batch, float* d_out, void* stream);
+
+/* Tile GEMM on the 5th-generation tensor cores (tcgen05, TMEM accumulator):
+ * d_d[128 x n] = d_a[128 x k] * d_b[n x k]^T with BF16 row-major inputs and an
+ * FP32 row-major output; n and k multiples of 16 in [16, 256]. The building
+ * block of the warm-start MLP, exported for testing. Synchronises `stream`. */
+int pbf_tc_gemm_bf16(const void* d_a, const void* d_b, float* d_d, int n, int k, void* stream);
 
 const char* pbf_last_error(void);
 int pbf_abi_version(void);

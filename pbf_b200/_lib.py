@@ -26,10 +26,12 @@ PBF_FLAG_WALL_DENSITY = 4
 FIELD = {
     "x": 0, "v": 1, "xold": 2, "xpred": 3, "xl": 4, "rho": 5, "dp": 6, "curl": 7, "vort": 8,
     "visc": 9, "cell": 10, "cell_start": 11, "perm": 12, "ncnt": 13, "nbr": 14, "hash": 15,
-    "lambda0": 16,
+    "lambda0": 16, "features": 17, "lambda_total": 18,
 }
 FLOAT4_FIELDS = {"x", "v", "xold", "xpred", "xl", "dp", "curl", "vort", "visc"}
-FLOAT_FIELDS = {"rho", "lambda0"}
+FLOAT_FIELDS = {"rho", "lambda0", "lambda_total"}
+MLP_NUM_WEIGHTS = 9280
+MLP_NUM_BIASES = 226
 
 
 class SolverParameter(C.Structure):
@@ -52,7 +54,7 @@ class ExtParams(C.Structure):
         ("cell_order", C.c_int), ("flags", C.c_uint), ("scorr_scale", C.c_float),
         ("sphere", C.c_float * 4), ("adaptive", C.c_int), ("density_tol", C.c_float),
         ("max_iterations", C.c_int), ("measure_error", C.c_int), ("debug", C.c_int),
-        ("warm_start", C.c_int), ("profile", C.c_int), ("block_size", C.c_int), ("reserved", C.c_int * 6),
+        ("warm_start", C.c_int), ("profile", C.c_int), ("block_size", C.c_int), ("record_features", C.c_int), ("reserved", C.c_int * 5),
     ]
 
 
@@ -104,6 +106,17 @@ _PROTOS = [
     ("pbf_stage_times", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int]),
     ("pbf_graph_kernel_count", C.c_int, [C.c_void_p]),
     ("pbf_measure_density_error", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
+    ("pbf_set_warm_start", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t]),
+    ("pbf_gather_training_rows", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pbf_mlp_trainer_create", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("pbf_mlp_trainer_destroy", C.c_int, [C.c_void_p]),
+    ("pbf_mlp_gradients", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]),
+    ("pbf_mlp_train_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p,
+                                     C.c_void_p]),
+    ("pbf_mlp_get_params", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pbf_mlp_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("pbf_tc_gemm_bf16", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     ("pbf_scan_workspace_bytes", C.c_size_t, [C.c_int]),
     ("pbf_scan_exclusive_i32", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
 ]

@@ -15,6 +15,7 @@
 
 #include "../../include/pbf.h"
 #include "pbf_kernels.h"
+#include "pbf_mlp.h"
 
 using namespace pbf;
 
@@ -84,12 +85,16 @@ struct pbf_solver {
     int *Sperm = nullptr, *Pperm = nullptr, *cell = nullptr, *ticket = nullptr, *tmp = nullptr,
         *cell_sorted = nullptr, *ncnt = nullptr, *nbr = nullptr, *cnt = nullptr, *cell_start = nullptr,
         *hash_dbg = nullptr;
-    float *lam_prev = nullptr, *lam_prev_sorted = nullptr, *lam0 = nullptr;
+    // total lambda of the substep (slot order), its copy permuted into the next
+    // substep's order, the last warm-start lambda0, and the 12 warm-start features
+    float *lam_acc = nullptr, *lam_prev_sorted = nullptr, *lam0 = nullptr, *feat = nullptr;
     void* scan_ws = nullptr;
     DevStats* dstats = nullptr;
     float* staging = nullptr;  // AoS float[3n] x2 for upload/download
     float* bound_pos = nullptr;
-    void* mlp = nullptr;  // learned warm start (not installed)
+    uint16_t* mlp_w = nullptr;  // installed warm-start weights (BF16) and biases/constants
+    float* mlp_b = nullptr;
+    int first_corrections = 0;  // corrections before the Jacobi loop (1 with features)
     // graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -178,8 +183,8 @@ template <typename T> int dalloc(T** p, size_t count) {
 void free_all(pbf_solver* s) {
     void* ptrs[] = {s->Sx, s->Sv, s->Px, s->Pv, s->Pxold, s->Q, s->omega, s->xpred_dbg, s->dp_dbg, s->vort_dbg,
                     s->visc_dbg, s->rho_dbg, s->Sperm, s->Pperm, s->cell, s->ticket, s->tmp, s->cell_sorted,
-                    s->ncnt, s->nbr, s->cnt, s->cell_start, s->hash_dbg, s->lam_prev, s->lam_prev_sorted, s->lam0,
-                    s->scan_ws, s->dstats, s->staging, s->scenes_d, s->sid};
+                    s->ncnt, s->nbr, s->cnt, s->cell_start, s->hash_dbg, s->lam_acc, s->lam_prev_sorted, s->lam0,
+                    s->feat, s->scan_ws, s->dstats, s->staging, s->scenes_d, s->sid, s->mlp_w, s->mlp_b};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->exec) cudaGraphExecDestroy(s->exec);
@@ -272,23 +277,47 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
     if (dbg) cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
     P(ST_SCAN, [&] { launch_scan(s->cnt, s->cell_start, s->nkeys, s->scan_ws, err, st); });
     P(ST_SCATTER, [&] { launch_scatter(n, s->cell, s->ticket, s->cell_start, s->tmp, err, st); });
+    // the substep's total lambda is tracked when features are computed (warm
+    // start, or recording features for training)
+    const bool warm = s->ext.warm_start && s->mlp_w;
+    const bool feats = warm || s->ext.record_features;
     P(ST_REORDER, [&] {
         launch_reorder(kp, true, s->Sx, s->Sv, s->Sperm, s->cell, s->cell_start, s->tmp, s->Px, s->Pv, s->Pxold,
-                       s->Pperm, s->cell_sorted, nullptr, nullptr, err, st);
+                       s->Pperm, s->cell_sorted, feats ? s->lam_acc : nullptr, feats ? s->lam_prev_sorted : nullptr,
+                       err, st);
     });
     if (dbg) launch_copy4(n, s->Px, s->xpred_dbg, st);
     P(ST_NEIGHBORS, [&] { launch_neighbors(kp, s->Px, s->cell_start, s->nbr, s->ncnt, st); });
 
     cudaMemsetAsync(ds, 0, offsetof(DevStats, err), st);  // per-substep slots; keeps the error bits
     const int iters = s->para.iterations;
-    const IterCtl fixed{};
+    float* acc = feats ? s->lam_acc : nullptr;
+    // First correction with features: the feature pass computes the plain lambda
+    // (and the 12 features); with a warm start the MLP replaces it by lambda0.
+    int first = 0;
+    if (feats && iters > 0) {
+        P(ST_LAMBDA, [&] {
+            launch_features(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->cell_start, s->lam_prev_sorted, s->Q, s->feat,
+                            s->lam_acc, st);
+        });
+        if (warm) P(ST_MLP, [&] { mlp_infer(s->mlp_w, s->mlp_b, s->feat, n, s->lam0, s->Q, s->lam_acc, err, st); });
+        const bool last = !s->ext.adaptive && iters == 1;
+        P(ST_DP, [&] {
+            launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, last ? s->Pv : nullptr, s->dp_dbg, IterCtl{},
+                      st);
+        });
+        first = 1;
+    }
+    s->first_corrections = first;
     if (!s->ext.adaptive) {
-        for (int it = 0; it < iters; ++it) {
+        for (int it = first; it < iters; ++it) {
             const bool last = it == iters - 1;
-            P(ST_LAMBDA, [&] { launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, fixed, st); });
+            IterCtl c{};
+            c.lam_acc = acc;
+            P(ST_LAMBDA, [&] { launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, c, st); });
             P(ST_DP, [&] {
-                launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, last ? s->Pv : nullptr, s->dp_dbg, fixed,
-                          st);
+                launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, last ? s->Pv : nullptr, s->dp_dbg,
+                          IterCtl{}, st);
             });
         }
         if (s->ext.measure_error)
@@ -297,13 +326,15 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
                                      nullptr, st);
             });
     } else {
-        // Iterate until the max density error is within tolerance. The graph
-        // holds max_iterations iterations; once converged the rest return at once.
+        // Iterate until the max density error is within tolerance (slot k holds
+        // the error after k corrections). The graph holds max_iterations
+        // iterations; once converged the rest return at once. Corrections beyond
+        // the configured count are the plain-iteration fallback.
         const int min_it = std::max(iters, 1);
         const int max_it = s->ext.max_iterations;
-        for (int it = 0; it < max_it; ++it) {
+        for (int it = first; it < max_it; ++it) {
             const IterCtl c{&ds->done, &ds->max_bits[it], &ds->sum[it], &ds->iters, &ds->conv_slot,
-                            (double)s->ext.density_tol, it, it >= min_it ? 1 : 0};
+                            (double)s->ext.density_tol, it, it >= min_it ? 1 : 0, acc};
             P(ST_LAMBDA, [&] { launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, c, st); });
             P(ST_DP, [&] { launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, nullptr, s->dp_dbg, c, st); });
         }
@@ -311,6 +342,7 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
         P(ST_MEASURE, [&] {
             launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[max_it], &ds->sum[max_it], &ds->done, st);
         });
+        launch_count_fallback(&ds->iters, first, iters, &ds->fallback, st);
         P(ST_VELOCITY, [&] { launch_velocity(kp, s->Px, s->Pxold, s->Pv, st); });
     }
     P(ST_CURL, [&] { launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, st); });
@@ -505,7 +537,8 @@ int create_common(const pbf_solver_parameter* para, int nscenes, const pbf_scene
     AL(s->nbr, (size_t)ext->max_neighbors * s->stride);
     AL(s->cnt, (size_t)s->nkeys);
     AL(s->cell_start, (size_t)s->nkeys + 1);
-    AL(s->lam_prev, n); AL(s->lam_prev_sorted, n); AL(s->lam0, n);
+    AL(s->lam_acc, n); AL(s->lam_prev_sorted, n); AL(s->lam0, n);
+    AL(s->feat, n * (size_t)MLP_IN);
     AL(s->staging, 6 * n);
     AL(s->dstats, 1);
     if (dbg) {
@@ -535,7 +568,7 @@ int create_common(const pbf_solver_parameter* para, int nscenes, const pbf_scene
         if (e == cudaSuccess) e = cudaMemcpy(s->sid, sid.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess) e = cudaMemset(s->dstats, 0, sizeof(DevStats));
-    if (e == cudaSuccess) e = cudaMemset(s->lam_prev, 0, sizeof(float) * n);
+    if (e == cudaSuccess) e = cudaMemset(s->lam_acc, 0, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaMemset(s->lam0, 0, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -568,7 +601,7 @@ int pbf_upload_device(pbf_solver* s, const float* d_pos, const float* d_vel, int
     CK(cudaMemsetAsync(s->dstats, 0, sizeof(DevStats), st));
     launch_from_aos(n, d_pos, d_vel, s->Sx, s->Sv, s->Sperm, &s->dstats->err, st);
     CK(cudaGetLastError());
-    CK(cudaMemsetAsync(s->lam_prev, 0, sizeof(float) * n, st));
+    CK(cudaMemsetAsync(s->lam_acc, 0, sizeof(float) * n, st));
     s->last_stream = st;
     s->uploaded = true;
     s->substeps = s->total_iters = s->fallbacks = 0;
@@ -599,7 +632,7 @@ int pbf_step(pbf_solver* s, int substeps, void* stream) {
     if (!s) return fail(PBF_ERR_INVALID, "null handle");
     if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_step before pbf_upload");
     if (substeps < 0) return fail(PBF_ERR_INVALID, "negative substep count");
-    if (s->ext.warm_start && !s->mlp) return fail(PBF_ERR_STATE, "warm_start set but no weights installed");
+    if (s->ext.warm_start && !s->mlp_w) return fail(PBF_ERR_STATE, "warm_start set but no weights installed");
     if (!s->exec) {
         int rc = build_graph(s);
         if (rc) return rc;
@@ -672,7 +705,7 @@ int pbf_get_stats(pbf_solver* s, pbf_stats* out) {
     out->error_bits = h.err;
     int slot = kSlots - 1;
     if (s->ext.adaptive) {
-        out->last_iterations = h.iters;
+        out->last_iterations = s->first_corrections + h.iters;
         slot = h.done ? h.conv_slot : s->ext.max_iterations;
     } else {
         out->last_iterations = s->para.iterations;
@@ -736,7 +769,8 @@ size_t pbf_field_bytes(const pbf_solver* s, int field) {
         case PBF_FIELD_X: case PBF_FIELD_V: case PBF_FIELD_XOLD: case PBF_FIELD_XPRED: case PBF_FIELD_XL:
         case PBF_FIELD_DP: case PBF_FIELD_CURL: case PBF_FIELD_VORT: case PBF_FIELD_VISC:
             return n * sizeof(float4);
-        case PBF_FIELD_RHO: case PBF_FIELD_LAMBDA0: return n * sizeof(float);
+        case PBF_FIELD_RHO: case PBF_FIELD_LAMBDA0: case PBF_FIELD_LAMBDA_TOTAL: return n * sizeof(float);
+        case PBF_FIELD_FEATURES: return n * MLP_IN * sizeof(float);
         case PBF_FIELD_CELL: case PBF_FIELD_PERM: case PBF_FIELD_NCNT: case PBF_FIELD_HASH: return n * sizeof(int);
         case PBF_FIELD_CELL_START: return ((size_t)s->nkeys + 1) * sizeof(int);
         case PBF_FIELD_NBR: return (size_t)s->ext.max_neighbors * s->stride * sizeof(int);
@@ -768,6 +802,8 @@ int pbf_fetch(pbf_solver* s, int field, void* dst, size_t bytes) {
         case PBF_FIELD_NBR: src = s->nbr; break;
         case PBF_FIELD_HASH: src = s->hash_dbg; break;
         case PBF_FIELD_LAMBDA0: src = s->lam0; break;
+        case PBF_FIELD_FEATURES: src = s->feat; break;
+        case PBF_FIELD_LAMBDA_TOTAL: src = s->lam_acc; break;
         default: break;
     }
     if (!src) return fail(PBF_ERR_STATE, "field %d is kept only when ext.debug is set", field);
@@ -781,6 +817,139 @@ int pbf_get_layout(const pbf_solver* s, int* ncells, int* stride, int* max_neigh
     if (ncells) *ncells = s->ncells;
     if (stride) *stride = s->stride;
     if (max_neighbors) *max_neighbors = s->ext.max_neighbors;
+    return PBF_OK;
+}
+
+int pbf_set_warm_start(pbf_solver* s, const unsigned short* w_bf16, size_t n_w, const float* b_f32, size_t n_b) {
+    if (!s || !w_bf16 || !b_f32) return fail(PBF_ERR_INVALID, "null argument");
+    if (n_w != (size_t)MLP_NUM_WEIGHTS || n_b != (size_t)MLP_NUM_BIASES)
+        return fail(PBF_ERR_INVALID, "warm start needs %d bf16 weights and %d floats", MLP_NUM_WEIGHTS,
+                    MLP_NUM_BIASES);
+    for (size_t i = 0; i < n_b; ++i)
+        if (!std::isfinite(b_f32[i])) return fail(PBF_ERR_NONFINITE, "non-finite warm-start constant %zu", i);
+    if (!s->mlp_w) {
+        int rc = dalloc(&s->mlp_w, (size_t)MLP_NUM_WEIGHTS);
+        if (!rc) rc = dalloc(&s->mlp_b, (size_t)MLP_NUM_BIASES);
+        if (rc) return rc;
+    }
+    CK(cudaMemcpy(s->mlp_w, w_bf16, sizeof(uint16_t) * MLP_NUM_WEIGHTS, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->mlp_b, b_f32, sizeof(float) * MLP_NUM_BIASES, cudaMemcpyHostToDevice));
+    if (s->exec) {  // the substep graph depends on whether a warm start is installed
+        cudaGraphExecDestroy(s->exec);
+        s->exec = nullptr;
+    }
+    return PBF_OK;
+}
+
+int pbf_gather_training_rows(pbf_solver* s, const int* d_slots, int count, float* d_feat, float* d_target,
+                             void* stream) {
+    if (!s || !d_slots || !d_feat || !d_target) return fail(PBF_ERR_INVALID, "null argument");
+    if (!s->ext.record_features && !s->ext.warm_start)
+        return fail(PBF_ERR_STATE, "features are kept only with ext.record_features or ext.warm_start");
+    if (count < 0) return fail(PBF_ERR_INVALID, "negative count");
+    cudaStream_t st = (cudaStream_t)stream;
+    launch_gather_rows(d_slots, count, s->n, s->feat, s->lam_acc, d_feat, d_target, &s->dstats->err, st);
+    CK(cudaGetLastError());
+    s->last_stream = st;
+    return PBF_OK;
+}
+
+struct pbf_mlp_trainer {
+    MlpTrainer* t;
+    int max_batch;
+};
+
+int pbf_mlp_trainer_create(int max_batch, const float* w32, const float* b32, pbf_mlp_trainer** out) {
+    if (!out || !w32 || !b32) return fail(PBF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (max_batch < 1 || max_batch > (1 << 24)) return fail(PBF_ERR_INVALID, "max_batch out of range");
+    for (int i = 0; i < MLP_NUM_WEIGHTS; ++i)
+        if (!std::isfinite(w32[i])) return fail(PBF_ERR_NONFINITE, "non-finite weight %d", i);
+    for (int i = 0; i < MLP_NUM_BIASES; ++i)
+        if (!std::isfinite(b32[i])) return fail(PBF_ERR_NONFINITE, "non-finite bias %d", i);
+    MlpTrainer* t = mlp_trainer_create(max_batch, w32, b32);
+    if (!t) return fail(PBF_ERR_ALLOC, "trainer buffers");
+    *out = new pbf_mlp_trainer{t, max_batch};
+    return PBF_OK;
+}
+
+int pbf_mlp_trainer_destroy(pbf_mlp_trainer* tr) {
+    if (!tr) return PBF_OK;
+    cudaDeviceSynchronize();
+    mlp_trainer_destroy(tr->t);
+    delete tr;
+    return PBF_OK;
+}
+
+int pbf_mlp_gradients(pbf_mlp_trainer* tr, const float* d_feat, const float* d_target, int batch, float* h_gw,
+                      float* h_gb, float* h_loss, void* stream) {
+    if (!tr || !d_feat || !d_target) return fail(PBF_ERR_INVALID, "null argument");
+    if (batch < 1 || batch > tr->max_batch) return fail(PBF_ERR_INVALID, "batch must lie in [1, max_batch]");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (mlp_gradients(tr->t, d_feat, d_target, batch, st)) return fail(PBF_ERR_CUDA, "gradient kernels failed");
+    if (h_gw || h_gb || h_loss) {
+        CK(cudaStreamSynchronize(st));
+        int err = 0;
+        mlp_read(tr->t, nullptr, nullptr, h_gw, h_gb, h_loss, &err);
+        if (err) return fail(PBF_ERR_DEVICE, "tensor-core pipeline error bits 0x%x", err);
+    }
+    return PBF_OK;
+}
+
+int pbf_mlp_train_step(pbf_mlp_trainer* tr, const float* d_feat, const float* d_target, int batch, float lr,
+                       float* h_loss, void* stream) {
+    int rc = pbf_mlp_gradients(tr, d_feat, d_target, batch, nullptr, nullptr, nullptr, stream);
+    if (rc) return rc;
+    if (!(lr > 0.0f) || !std::isfinite(lr)) return fail(PBF_ERR_INVALID, "learning rate must be positive");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (mlp_adam(tr->t, lr, 0.9f, 0.999f, 1e-8f, st)) return fail(PBF_ERR_CUDA, "Adam kernels failed");
+    if (h_loss) {
+        CK(cudaStreamSynchronize(st));
+        int err = 0;
+        mlp_read(tr->t, nullptr, nullptr, nullptr, nullptr, h_loss, &err);
+        if (err) return fail(PBF_ERR_DEVICE, "tensor-core pipeline error bits 0x%x", err);
+    }
+    return PBF_OK;
+}
+
+int pbf_mlp_get_params(pbf_mlp_trainer* tr, float* w32, float* b32, unsigned short* w_bf16) {
+    if (!tr) return fail(PBF_ERR_INVALID, "null handle");
+    CK(cudaDeviceSynchronize());
+    mlp_read(tr->t, w32, b32, nullptr, nullptr, nullptr, nullptr);
+    if (w_bf16)
+        CK(cudaMemcpy(w_bf16, mlp_weights_bf16(tr->t), sizeof(uint16_t) * MLP_NUM_WEIGHTS, cudaMemcpyDeviceToHost));
+    return PBF_OK;
+}
+
+int pbf_mlp_forward(pbf_mlp_trainer* tr, const float* d_feat, int batch, float* d_out, void* stream) {
+    if (!tr || !d_feat || !d_out) return fail(PBF_ERR_INVALID, "null argument");
+    if (batch < 1) return fail(PBF_ERR_INVALID, "batch must be positive");
+    static int* d_err = nullptr;
+    if (!d_err) CK(cudaMalloc(&d_err, sizeof(int)));
+    cudaStream_t st = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    if (mlp_infer(mlp_weights_bf16(tr->t), mlp_biases(tr->t), d_feat, batch, d_out, nullptr, nullptr, d_err, st))
+        return fail(PBF_ERR_CUDA, "inference kernel failed");
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h) return fail(PBF_ERR_DEVICE, "tensor-core pipeline error bits 0x%x", h);
+    return PBF_OK;
+}
+
+int pbf_tc_gemm_bf16(const void* d_a, const void* d_b, float* d_d, int n, int k, void* stream) {
+    if (!d_a || !d_b || !d_d) return fail(PBF_ERR_INVALID, "null argument");
+    if (n < 16 || n > 256 || n % 16 || k < 16 || k > 256 || k % 16)
+        return fail(PBF_ERR_INVALID, "n and k must be multiples of 16 in [16, 256]");
+    static int* d_err = nullptr;
+    if (!d_err) CK(cudaMalloc(&d_err, sizeof(int)));
+    cudaStream_t st = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    if (tc_gemm_bf16(d_a, d_b, d_d, n, k, d_err, st)) return fail(PBF_ERR_CUDA, "tensor-core GEMM launch failed");
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (h) return fail(PBF_ERR_DEVICE, "tensor-core pipeline wait expired (error bits 0x%x)", h);
     return PBF_OK;
 }
 

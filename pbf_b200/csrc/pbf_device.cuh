@@ -88,6 +88,8 @@ struct IterCtl {
     double tol;
     int slot;
     int may_stop;                  // 0 while below the minimum iteration count
+    float* lam_acc;                // when set, the lambda pass adds its lambda here (the
+                                   // substep's total lambda: warm-start feature and target)
 };
 
 // ---- deterministic sine ------------------------------------------------------

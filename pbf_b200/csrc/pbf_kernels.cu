@@ -362,9 +362,135 @@ __global__ void __launch_bounds__(256, 6) k_lambda(KParams p, const float4* __re
         gm = __fdiv_rn(gm, p.rho0sq);
         const float lam = __fdiv_rn(-C, gm + p.eps);
         xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
+        if (ctl.lam_acc) ctl.lam_acc[k] += lam;
         if (DEBUG) rho_out[k] = rho;
     }
     if (ctl.max_bits) block_error_reduce(err, ctl.max_bits, ctl.sum);
+}
+
+// ---------------------------------------------------------------------------
+// a17: warm-start features (no reference counterpart), computed in the first
+// lambda pass of a substep together with that pass's lambda (the same
+// arithmetic as k_lambda, so recording features changes no result):
+//   0 neighbour count / cap         1 fluid density / rho0
+//   2 previous substep's total lambda
+//   3 sum |grad C|^2 (the lambda denominator without eps)
+//   4 velocity divergence sum (v_j - v_i) . grad W / rho0 (predicted velocities)
+//   5-7 distance to the nearer wall per axis / h, clamped to [0, 4]
+//   8-11 occupancy of the 27 cells around the particle's cell: own cell, mean,
+//        fraction non-empty, maximum
+// lam_acc starts the substep's total lambda at this pass's lambda.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_features(KParams p, const float4* __restrict__ x,
+                                                  const float4* __restrict__ v, const int* __restrict__ nbr,
+                                                  const int* __restrict__ ncnt, const int* __restrict__ cell_start,
+                                                  const float* __restrict__ lam_prev, float4* __restrict__ xl,
+                                                  float* __restrict__ feat, float* __restrict__ lam_acc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= p.n) return;
+    const SceneView sc = scene_of(p, k);
+    const f3 xk = make3(x[k]);
+    const f3 vk = make3(v[k]);
+    const int cnt = ncnt[k];
+    float rho = 0.0f, gm = 0.0f, div = 0.0f;
+    f3 gs = {0.0f, 0.0f, 0.0f};
+    for (int q0 = 0; q0 < cnt; q0 += NB) {
+        int jj[NB];
+        load_idx(p, nbr, k, q0, cnt, jj);
+        float4 xj[NB], vj[NB];
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            xj[u] = x[jj[u]];
+            vj[u] = v[jj[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            if (q0 + u >= cnt) break;
+            const f3 r = sub3(xk, make3(xj[u]));
+            const float r2 = dot_fma(r, r);
+            rho = rho + w_poly6(p, r2);
+            const f3 g = grad_spiky(p, r, r2);
+            gs = {gs.x + g.x, gs.y + g.y, gs.z + g.z};
+            gm = __fmaf_rn(g.x, g.x, gm);
+            gm = __fmaf_rn(g.y, g.y, gm);
+            gm = __fmaf_rn(g.z, g.z, gm);
+            const f3 vji = sub3(make3(vj[u]), vk);
+            div = __fmaf_rn(vji.x, g.x, div);
+            div = __fmaf_rn(vji.y, g.y, div);
+            div = __fmaf_rn(vji.z, g.z, div);
+        }
+    }
+    const float rho_fluid = rho;
+    if (p.flags & FLAG_WALL_DENSITY) {
+        f3 gw;
+        rho = rho + wall_term(p, sc, xk, gw);
+        gs = {gs.x + gw.x, gs.y + gw.y, gs.z + gw.z};
+    }
+    float C = __fdiv_rn(rho, p.rho0) - 1.0f;
+    if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
+    gm = __fmaf_rn(gs.x, gs.x, gm);
+    gm = __fmaf_rn(gs.y, gs.y, gm);
+    gm = __fmaf_rn(gs.z, gs.z, gm);
+    gm = __fdiv_rn(gm, p.rho0sq);
+    const float lam = __fdiv_rn(-C, gm + p.eps);
+    xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
+    lam_acc[k] = lam;
+
+    float f[12];
+    f[0] = (float)cnt / (float)p.max_nbr;
+    f[1] = rho_fluid / p.rho0;
+    f[2] = lam_prev[k];
+    f[3] = gm;
+    f[4] = div / p.rho0;
+    const float qa[3] = {xk.x, xk.y, xk.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float dw = fminf(qa[a] - sc.bmin[a], sc.bmax[a] - qa[a]) * p.inv_h;
+        f[5 + a] = fminf(fmaxf(dw, 0.0f), 4.0f);
+    }
+    int d[3];
+    cell_dims(p, sc, xk, d);
+    int own = 0, tot = 0, nonempty = 0, mx = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int cx = d[0] + dx, cy = d[1] + dy, cz = d[2] + dz;
+                if (cx < 0 || cy < 0 || cz < 0 || cx >= sc.dims[0] || cy >= sc.dims[1] || cz >= sc.dims[2]) continue;
+                const int c = sc.cell_base + cx + cy * sc.dims[0] + cz * sc.dims[0] * sc.dims[1];
+                const int occ = cell_start[c + 1] - cell_start[c];
+                if (dx == 0 && dy == 0 && dz == 0) own = occ;
+                tot += occ;
+                nonempty += occ > 0;
+                mx = max(mx, occ);
+            }
+    f[8] = (float)own;
+    f[9] = (float)tot / 27.0f;
+    f[10] = (float)nonempty / 27.0f;
+    f[11] = (float)mx;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) feat[(size_t)k * 12 + i] = f[i];
+}
+
+// Copies features and total lambda of the given slots (training rows).
+__global__ void k_gather_rows(const int* __restrict__ slots, int count, int n, const float* __restrict__ feat,
+                              const float* __restrict__ lam_acc, float* __restrict__ out_feat,
+                              float* __restrict__ out_target, int* __restrict__ err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int s = slots[i];
+    if (s < 0 || s >= n) {
+        atomicOr(err, DEVERR_BAD_INDEX);
+        return;
+    }
+#pragma unroll
+    for (int c = 0; c < 12; ++c) out_feat[(size_t)i * 12 + c] = feat[(size_t)s * 12 + c];
+    out_target[i] = lam_acc[s];
+}
+
+// Counts a substep as a fallback when the adaptive loop needed more corrections
+// than the configured iteration count.
+__global__ void k_count_fallback(const int* __restrict__ iters, int first, int configured, int* __restrict__ fallback) {
+    if (first + *iters > configured) *fallback += 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -684,6 +810,24 @@ void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, c
     const int b = blocks_for(p.n, p.block);
     if (debug) k_dp<true><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
     else k_dp<false><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+}
+
+void launch_features(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
+                     const int* cell_start, const float* lam_prev, float4* xl, float* feat, float* lam_acc,
+                     cudaStream_t st) {
+    k_features<<<blocks_for(p.n, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, cell_start, lam_prev, xl, feat,
+                                                              lam_acc);
+}
+
+void launch_gather_rows(const int* slots, int count, int n, const float* feat, const float* lam_acc, float* out_feat,
+                        float* out_target, int* err, cudaStream_t st) {
+    if (count > 0)
+        k_gather_rows<<<blocks_for(count, 256), 256, 0, st>>>(slots, count, n, feat, lam_acc, out_feat, out_target,
+                                                               err);
+}
+
+void launch_count_fallback(const int* iters, int first, int configured, int* fallback, cudaStream_t st) {
+    k_count_fallback<<<1, 1, 0, st>>>(iters, first, configured, fallback);
 }
 
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st) {

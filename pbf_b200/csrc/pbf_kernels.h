@@ -23,6 +23,12 @@ void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr
                    float* rho, const IterCtl& ctl, cudaStream_t st);
 void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, const int* ncnt, const float4* xold,
                float4* xout, float4* vout, float4* dp, const IterCtl& ctl, cudaStream_t st);
+void launch_features(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
+                     const int* cell_start, const float* lam_prev, float4* xl, float* feat, float* lam_acc,
+                     cudaStream_t st);
+void launch_gather_rows(const int* slots, int count, int n, const float* feat, const float* lam_acc, float* out_feat,
+                        float* out_target, int* err, cudaStream_t st);
+void launch_count_fallback(const int* iters, int first, int configured, int* fallback, cudaStream_t st);
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st);
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
                  cudaStream_t st);

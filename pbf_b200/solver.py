@@ -158,6 +158,8 @@ class Solver:
         nbytes = lib().pbf_field_bytes(self._h, fid)
         if name in _lib.FLOAT4_FIELDS:
             out = np.empty((self.n, 4), np.float32)
+        elif name == "features":
+            out = np.empty((self.n, 12), np.float32)
         elif name in _lib.FLOAT_FIELDS:
             out = np.empty(self.n, np.float32)
         else:
