@@ -261,6 +261,19 @@ int pbf_mlp_forward(pbf_mlp_trainer* t, const float* d_feat, int batch, float* d
  * block of the warm-start MLP, exported for testing. Synchronises `stream`. */
 int pbf_tc_gemm_bf16(const void* d_a, const void* d_b, float* d_d, int n, int k, void* stream);
 
+/* The same exclusive scan for callers that cannot allocate device memory (no
+ * counterpart in the reference). A render or simulation loop that must not
+ * stall on cudaMalloc, or a plug-in whose host application owns every device
+ * allocation, has no workspace to pass; this variant keeps its scratch (about
+ * 33 KB) in a device array inside the library, so it calls no cudaMalloc,
+ * cudaFree or allocating library routine. Limit: n <= 16,777,216 (larger n is
+ * rejected with PBF_ERR_INVALID). The first call on each device looks up the
+ * array's device address, so make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race, so issue them
+ * on one stream or serialise them. d_out receives n + 1 ints (total last);
+ * the input is left unchanged. Synchronises `stream`. */
+int pbf_scan_exclusive_i32_noalloc(const int* d_in, int* d_out, int n, void* stream);
+
 const char* pbf_last_error(void);
 int pbf_abi_version(void);
 

@@ -119,6 +119,7 @@ _PROTOS = [
     ("pbf_tc_gemm_bf16", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     ("pbf_scan_workspace_bytes", C.c_size_t, [C.c_int]),
     ("pbf_scan_exclusive_i32", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
+    ("pbf_scan_exclusive_i32_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
 ]
 
 

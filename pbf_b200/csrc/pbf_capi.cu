@@ -34,6 +34,15 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
+}  // namespace
+
+int pbf::set_last_error(int code, const char* msg) {
+    g_err = msg ? msg : "";
+    return code;
+}
+
+namespace {
+
 #define CK(call)                                                                              \
     do {                                                                                      \
         cudaError_t e_ = (call);                                                              \
