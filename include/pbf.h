@@ -84,7 +84,9 @@ typedef struct pbf_ext_params {
     int profile;         /* 1: time every launch with CUDA events (pbf_stage_times) */
     int block_size;      /* threads per block of the neighbour passes: 0 (= 256), 64, 128 or 256 */
     int record_features; /* 1: keep warm-start features and total lambda (training data) */
-    int reserved[5];
+    float warm_clamp;    /* warm start: lambda0 keeps the sign of the plain lambda of its
+                            pass and at most warm_clamp times its magnitude (default 4; 0: off) */
+    int reserved[4];
 } pbf_ext_params;
 
 typedef struct pbf_stats {

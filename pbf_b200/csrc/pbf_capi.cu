@@ -249,6 +249,7 @@ int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, co
     if (e->adaptive && p->iterations > e->max_iterations)
         return fail(PBF_ERR_INVALID, "iterations exceeds max_iterations");
     if (!std::isfinite(e->density_tol) || e->density_tol < 0) return fail(PBF_ERR_INVALID, "density_tol must be >= 0");
+    if (!std::isfinite(e->warm_clamp) || e->warm_clamp < 0) return fail(PBF_ERR_INVALID, "warm_clamp must be >= 0");
     return PBF_OK;
 }
 
@@ -309,7 +310,10 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
             launch_features(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->cell_start, s->lam_prev_sorted, s->Q, s->feat,
                             s->lam_acc, st);
         });
-        if (warm) P(ST_MLP, [&] { mlp_infer(s->mlp_w, s->mlp_b, s->feat, n, s->lam0, s->Q, s->lam_acc, err, st); });
+        if (warm)
+            P(ST_MLP, [&] {
+                mlp_infer(s->mlp_w, s->mlp_b, s->feat, n, s->lam0, s->Q, s->lam_acc, s->ext.warm_clamp, err, st);
+            });
         const bool last = !s->ext.adaptive && iters == 1;
         P(ST_DP, [&] {
             launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, last ? s->Pv : nullptr, s->dp_dbg, IterCtl{},
@@ -431,6 +435,7 @@ void pbf_ext_params_default(pbf_ext_params* e) {
     e->scorr_scale = 1.0f;
     e->density_tol = 0.01f;
     e->max_iterations = 16;
+    e->warm_clamp = 4.0f;
 }
 
 int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], const float boundary[6],
@@ -937,7 +942,8 @@ int pbf_mlp_forward(pbf_mlp_trainer* tr, const float* d_feat, int batch, float* 
     if (!d_err) CK(cudaMalloc(&d_err, sizeof(int)));
     cudaStream_t st = (cudaStream_t)stream;
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-    if (mlp_infer(mlp_weights_bf16(tr->t), mlp_biases(tr->t), d_feat, batch, d_out, nullptr, nullptr, d_err, st))
+    if (mlp_infer(mlp_weights_bf16(tr->t), mlp_biases(tr->t), d_feat, batch, d_out, nullptr, nullptr, 0.0f, d_err,
+                  st))
         return fail(PBF_ERR_CUDA, "inference kernel failed");
     int h = 0;
     CK(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -451,18 +451,27 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
     int d[3];
     cell_dims(p, sc, xk, d);
     int own = 0, tot = 0, nonempty = 0, mx = 0;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int cx = d[0] + dx, cy = d[1] + dy, cz = d[2] + dz;
-                if (cx < 0 || cy < 0 || cz < 0 || cx >= sc.dims[0] || cy >= sc.dims[1] || cz >= sc.dims[2]) continue;
-                const int c = sc.cell_base + cx + cy * sc.dims[0] + cz * sc.dims[0] * sc.dims[1];
-                const int occ = cell_start[c + 1] - cell_start[c];
-                if (dx == 0 && dy == 0 && dz == 0) own = occ;
-                tot += occ;
-                nonempty += occ > 0;
-                mx = max(mx, occ);
+    // nine rows of three x-adjacent cells; a row's counts are differences of
+    // consecutive cell starts (keys are x-fastest)
+    const int x0 = max(d[0] - 1, 0), x1 = min(d[0] + 1, sc.dims[0] - 1);
+    if (x0 <= x1) {
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int cy = d[1] + dy, cz = d[2] + dz;
+                if (cy < 0 || cz < 0 || cy >= sc.dims[1] || cz >= sc.dims[2]) continue;
+                const int row = sc.cell_base + cy * sc.dims[0] + cz * sc.dims[0] * sc.dims[1];
+                int prev = cell_start[row + x0];
+                for (int cx = x0; cx <= x1; ++cx) {
+                    const int next = cell_start[row + cx + 1];
+                    const int occ = next - prev;
+                    prev = next;
+                    if (cx == d[0] && dy == 0 && dz == 0) own = occ;
+                    tot += occ;
+                    nonempty += occ > 0;
+                    mx = max(mx, occ);
+                }
             }
+    }
     f[8] = (float)own;
     f[9] = (float)tot / 27.0f;
     f[10] = (float)nonempty / 27.0f;

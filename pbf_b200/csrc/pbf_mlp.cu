@@ -91,14 +91,23 @@ int tc_gemm_bf16(const void* A, const void* B, float* D, int N, int K, int* err,
 constexpr float GELU_C = 0.7978845608028654f;  // sqrt(2 / pi)
 constexpr float GELU_A = 0.044715f;
 
+// hardware tanh (one MUFU operation, about 2^-11 relative error: below the BF16
+// rounding the activations go through anyway)
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// GELU, tanh form: 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))
 __device__ __forceinline__ float gelu(float z) {
     const float u = GELU_C * (z + GELU_A * z * z * z);
-    return 0.5f * z * (1.0f + tanhf(u));
+    return 0.5f * z * (1.0f + tanh_fast(u));
 }
 
 __device__ __forceinline__ float gelu_grad(float z) {
     const float u = GELU_C * (z + GELU_A * z * z * z);
-    const float t = tanhf(u);
+    const float t = tanh_fast(u);
     return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * GELU_C * (1.0f + 3.0f * GELU_A * z * z);
 }
 
@@ -173,6 +182,7 @@ struct FwdIO {
     float* out;
     float4* q;
     float* lam_acc;
+    float clamp;  // trust-region factor around q.w (0: none)
     // training
     const float* target;  // [n]
     float inv_batch;
@@ -326,7 +336,14 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
         }
         if (!TRAIN) {
             if (valid) {
-                const float lam0 = y * sb[OSCALE_OFF];
+                float lam0 = y * sb[OSCALE_OFF];
+                if (io.q && io.clamp > 0.0f) {
+                    // trust region around the plain lambda of the same pass (q.w):
+                    // same sign, at most clamp times its magnitude
+                    const float lp = reinterpret_cast<const float*>(io.q)[4 * (size_t)row + 3];
+                    const float a = io.clamp * lp;
+                    lam0 = fminf(fmaxf(lam0, fminf(a, 0.0f)), fmaxf(a, 0.0f));
+                }
                 if (io.out) io.out[row] = lam0;
                 if (io.q) reinterpret_cast<float*>(io.q)[4 * (size_t)row + 3] = lam0;
                 if (io.lam_acc) io.lam_acc[row] = lam0;
@@ -509,7 +526,7 @@ static int sm_count() {
 }
 
 int mlp_infer(const uint16_t* w_bf16, const float* b, const float* feat, int n, float* out, float4* q, float* lam_acc,
-              int* err, cudaStream_t st) {
+              float clamp, int* err, cudaStream_t st) {
     if (n <= 0) return 0;
     static bool attr = false;
     if (!attr) {
@@ -526,9 +543,12 @@ int mlp_infer(const uint16_t* w_bf16, const float* b, const float* feat, int n, 
     io.out = out;
     io.q = q;
     io.lam_acc = lam_acc;
+    io.clamp = clamp;
     io.err = err;
+    // four CTAs per SM (54 KB of shared memory and 128 TMEM columns each) overlap
+    // one another's tensor-core waits
     const int tiles = (n + TILE - 1) / TILE;
-    const int grid = tiles < sm_count() ? tiles : sm_count();
+    const int grid = tiles < 4 * sm_count() ? tiles : 4 * sm_count();
     k_mlp_fwd<false><<<grid, 128, FWD_SMEM_INFER, st>>>(io);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -38,9 +38,11 @@ constexpr int MLP_NUM_TRAINED_BIASES = 193;  // b1, b2, b3, b4
 int tc_gemm_bf16(const void* A, const void* B, float* D, int N, int K, int* err, cudaStream_t st);
 
 // Inference: lambda0 for `n` rows of raw features feat[n][12]. Writes lambda0 to
-// out (if not null), to q[k].w (if not null) and to lam_acc (if not null).
+// out (if not null), to q[k].w (if not null) and to lam_acc (if not null). With q
+// and clamp > 0, lambda0 is kept to the sign of the plain lambda in q[k].w and
+// to at most clamp times its magnitude.
 int mlp_infer(const uint16_t* w_bf16, const float* b, const float* feat, int n, float* out, float4* q,
-              float* lam_acc, int* err, cudaStream_t st);
+              float* lam_acc, float clamp, int* err, cudaStream_t st);
 
 struct MlpTrainer;
 MlpTrainer* mlp_trainer_create(int max_batch, const float* w32, const float* b32);
