@@ -336,6 +336,8 @@ def run_b200(args) -> int:
     plain_ref = {"value": value, "ext_kw": ext_kw, "state": (state_pos, state_vel),
                  "batched_tune": (out["batched"]["autotune"]["cell_scale"], out["batched"]["autotune"]["block_size"])}
     out["learned"] = measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, plain_ref)
+    weights = out["learned"].pop("_weights")
+    out["large"] = measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, weights)
     if rank == 0 and world == 1:
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0:
@@ -462,6 +464,39 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
     b.close()
     out["speedup_learned_batched_vs_plain"] = out["batched"]["value"] / plain["value"]
     out["speedup_learned_vs_plain"] = out["single"]["value"] / plain["value"]
+    out["_weights"] = (w16, b32)
+    return out
+
+
+def measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, weights) -> dict:
+    """The 4,194,304-particle double dam break (two 128^3 blocks, sphere of radius
+    20h at the centre of a 320h x 160h x 160h box) batched with 8 scenes of
+    65,536 particles: plain 4 iterations, and the learned warm start with 2
+    iterations plus the adaptive plain fallback up to 16 iterations while the
+    max density error exceeds 10 %."""
+    from pbf_b200 import BatchSolver, learned, multigpu, scenes
+    out = {"workload": "double dam break 2 x 128^3 + sphere r=20h, box 320h x 160h x 160h, + 8 x 65,536"}
+    w16, b32 = weights
+    for label, iters, kw in (("plain", 4, {}),
+                             ("learned_adaptive", 2, {"warm_start": 1, "adaptive": 1, "density_tol": 0.1,
+                                                      "max_iterations": 16})):
+        scs = scenes.config4(seed=0, iterations=iters)
+        parts = multigpu.assign_scenes([x.n for x in scs], world)
+        mine = [scs[i] for i in parts[rank]]
+        para, descs, ov, pos, vel = scenes.batch_inputs(mine, iterations=iters)
+        ov.update(kw)
+        b = BatchSolver(para, descs, scenes.default_ext(**ov))
+        if kw.get("warm_start"):
+            learned.install(b, w16, b32)
+        b.upload(pos, vel)
+        b.step(max(args.warmup, 3), stream)
+        t, err = _timed_errors(b, args.steps, flush, stream, barrier, max_over_ranks)
+        total = sum(x.n for x in scs)
+        st = b.stats()
+        out[label] = {"iterations": iters, "particles": total, "value": total * args.steps / t, "unit": UNIT,
+                      "ms_per_step": 1e3 * t / args.steps, "density_error": err,
+                      "last_iterations": st["last_iterations"], "fallbacks": st["fallbacks"]}
+        b.close()
     return out
 
 
