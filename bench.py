@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark: particle-substeps/s of the PBF solver step on B200.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--legs all|main|...]
 
 Workload (one step = one PBF substep): the 262,144-particle dam break (64^3
 lattice at spacing 0.5h with +-0.01h seeded jitter, h = 0.1, box 80h x 40h x
@@ -214,7 +214,7 @@ def run_b200(args) -> int:
     stream = torch.cuda.current_stream()
     tuned = autotune.tune([sc], iterations=4)
     ext_kw = dict(grid_dims=autotune.dims_for_scale(sc.ext_overrides["grid_dims"], tuned["cell_scale"]),
-                  cell_scale=tuned["cell_scale"], block_size=tuned["block_size"])
+                  **autotune.ext_for(tuned))
     solver = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(**ext_kw))
     solver.upload(sc.pos, sc.vel)
     kernels = solver.kernel_count()
@@ -323,7 +323,7 @@ def run_b200(args) -> int:
                           "frac_hbm": step_bytes / (tot_s / args.steps) / 1e9 / hbm_peak},
         "stages_ms": {k: round(v, 5) for k, v in stages.items()},
         "stages_note": "per-kernel CUDA-event times from a profiled pass over the same K substeps and state",
-        "autotune": {"cell_scale": tuned["cell_scale"], "block_size": tuned["block_size"], "table": tuned["table"]},
+        "autotune": dict(autotune.ext_for(tuned), table=tuned["table"]),
         "value_l2_warm": n * world * args.steps / warm_s,
         "density_error": {"max": statistics.mean(e[0] for e in errs), "worst": max(e[0] for e in errs),
                           "mean": statistics.mean(e[1] for e in errs), "target_max": 0.01,
@@ -332,13 +332,17 @@ def run_b200(args) -> int:
                                   "worst = its largest value; mean = mean over particles and substeps"},
         "clocks": clocks,
     }
-    out["batched"] = measure_batched(args, rank, world, dev, flush, stream, barrier, max_over_ranks)
-    plain_ref = {"value": value, "ext_kw": ext_kw, "state": (state_pos, state_vel),
-                 "batched_tune": (out["batched"]["autotune"]["cell_scale"], out["batched"]["autotune"]["block_size"])}
-    out["learned"] = measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, plain_ref)
-    weights = out["learned"].pop("_weights")
-    out["large"] = measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, weights)
-    if rank == 0 and world == 1:
+    legs = set(args.legs.split(","))
+    if legs & {"all", "batched", "learned", "large"}:
+        out["batched"] = measure_batched(args, rank, world, dev, flush, stream, barrier, max_over_ranks)
+    if legs & {"all", "learned", "large"}:
+        plain_ref = {"value": value, "ext_kw": ext_kw, "state": (state_pos, state_vel),
+                     "batched_tune": autotune.ext_for(out["batched"]["autotune"])}
+        out["learned"] = measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, plain_ref)
+        weights = out["learned"].pop("_weights")
+        if legs & {"all", "large"}:
+            out["large"] = measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, weights)
+    if rank == 0 and world == 1 and legs & {"all", "cpu"}:
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0:
         print(json.dumps(out))
@@ -362,7 +366,7 @@ def measure_batched(args, rank, world, dev, flush, stream, barrier, max_over_ran
     para, descs, ov, pos, vel = scenes.batch_inputs(mine, iterations=4)
     for d in descs:
         d["grid_dims"] = autotune.dims_for_scale(d["grid_dims"], tuned["cell_scale"])
-    ov.update(cell_scale=tuned["cell_scale"], block_size=tuned["block_size"])
+    ov.update(autotune.ext_for(tuned))
     b = BatchSolver(para, descs, scenes.default_ext(**ov))
     b.upload(pos, vel)
     b.step(max(args.warmup, 3), stream)
@@ -383,8 +387,7 @@ def measure_batched(args, rank, world, dev, flush, stream, barrier, max_over_ran
     out = {"workload": "64 scenes, counts log-uniform in [4096, 65536] (seed 0), box aspect U[1,3], 4 iterations",
            "scenes": len(scs), "particles": total, "value": total * args.steps / t, "unit": UNIT,
            "ms_per_step": 1e3 * t / args.steps, "kernels_per_step": b.kernel_count(),
-           "autotune": {"cell_scale": tuned["cell_scale"], "block_size": tuned["block_size"],
-                        "table": tuned["table"]},
+           "autotune": dict(autotune.ext_for(tuned), table=tuned["table"]),
            "density_error": {"max": max(e[0] for e in errs), "mean": statistics.mean(e[1] for e in errs)}}
     b.close()
     return out
@@ -448,10 +451,10 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
     parts = multigpu.assign_scenes([x.n for x in scs], world)
     mine = [scs[i] for i in parts[rank]]
     para, descs, ov, pos, vel = scenes.batch_inputs(mine, iterations=2)
-    cs, bs = plain["batched_tune"]
+    bt = plain["batched_tune"]
     for d in descs:
-        d["grid_dims"] = autotune.dims_for_scale(d["grid_dims"], cs)
-    ov.update(cell_scale=cs, block_size=bs, warm_start=1)
+        d["grid_dims"] = autotune.dims_for_scale(d["grid_dims"], bt["cell_scale"])
+    ov.update(bt, warm_start=1)
     b = BatchSolver(para, descs, scenes.default_ext(**ov))
     learned.install(b, w16, b32)
     b.upload(pos, vel)
@@ -516,6 +519,9 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--legs", default="all",
+                    help="comma list of legs after the single-scene one: all, batched, learned, large, cpu "
+                         "(main = the single-scene leg alone)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -32,7 +32,7 @@ class OracleParams(C.Structure):
         ("bmin", C.c_float * 3), ("bmax", C.c_float * 3), ("wall_jitter", C.c_float), ("grad_rmin", C.c_float),
         ("max_nbr", C.c_int), ("formulation", C.c_int), ("arith", C.c_int), ("cell_order", C.c_int),
         ("reorder", C.c_int), ("flags", C.c_int), ("scorr_scale", C.c_float), ("sphere", C.c_float * 4),
-        ("wall_jitter_d", C.c_double), ("cell_scale", C.c_float),
+        ("wall_jitter_d", C.c_double), ("cell_scale", C.c_float), ("lanes", C.c_int),
     ]
 
 
@@ -66,8 +66,10 @@ def olib() -> C.CDLL:
 
 def params_from(para, grid_space, boundary, *, gravity=(0.0, -49.0, 0.0), dims=(64, 64, 64), formulation=0,
                 arith=1, cell_order=0, reorder=1, flags=0, scorr_scale=1.0, wall_jitter=None, grad_rmin=0.01,
-                max_nbr=63, sphere=(0, 0, 0, 0), cell_scale=1.0, iterations=None) -> OracleParams:
-    """Oracle parameters from a SolverParameter-like object and the two AABBs."""
+                max_nbr=63, sphere=(0, 0, 0, 0), cell_scale=1.0, iterations=None, lanes=4) -> OracleParams:
+    """Oracle parameters from a SolverParameter-like object and the two AABBs.
+    lanes: pair lanes per particle of the product arithmetic (the library's
+    pair_lanes, default 4)."""
     p = OracleParams()
     for f in ("h", "restRho", "epsilon", "k", "n", "deltaq", "c", "dt"):
         setattr(p, f, float(getattr(para, f)))
@@ -94,6 +96,7 @@ def params_from(para, grid_space, boundary, *, gravity=(0.0, -49.0, 0.0), dims=(
     for a in range(4):
         p.sphere[a] = sphere[a]
     p.cell_scale = cell_scale
+    p.lanes = lanes
     return p
 
 
@@ -107,7 +110,7 @@ def params_for_scene(scene, ext=None, **kw) -> OracleParams:
                        scorr_scale=ov.get("scorr_scale", 1.0), wall_jitter=ov.get("wall_jitter", 0.01),
                        grad_rmin=ov.get("grad_rmin", 0.01), max_nbr=ov.get("max_neighbors", 63),
                        sphere=ov.get("sphere", (0, 0, 0, 0)), cell_scale=ov.get("cell_scale", 1.0),
-                       cell_order=ov.get("cell_order", 0), **kw)
+                       cell_order=ov.get("cell_order", 0), lanes=kw.pop("lanes", ov.get("pair_lanes", 0) or 4), **kw)
 
 
 class Oracle:

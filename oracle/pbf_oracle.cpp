@@ -54,6 +54,7 @@ typedef struct oracle_params {
     float sphere[4];      // static sphere obstacle centre xyz, radius (radius<=0: none)
     double wall_jitter_d; // the GPU reference's RANDOM_OFFSET_COEFF is the double literal 0.01
     float cell_scale;     // grid cell edge = h * cell_scale (reference: 1)
+    int lanes;            // product: pair lanes per particle (1, 2, 4 or 8; <= 1: one lane)
 } oracle_params;
 
 enum {
@@ -110,6 +111,22 @@ template <typename T> struct V3 {
     T x, y, z;
 };
 template <typename T> inline V3<T> sub(const V3<T>& a, const V3<T>& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <typename T> inline V3<T> add(const V3<T>& a, const V3<T>& b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+
+// product: the CUDA library splits a particle's neighbour list over L pair lanes
+// (lane t takes entries t, t+L, t+2L, ... in list order) and combines the lane
+// sums by an xor butterfly over distances 1, 2, 4, i.e. ((a0+a1)+(a2+a3))+... .
+constexpr int kMaxLanes = 8;
+template <typename T> inline T combine_lanes(T* a, int L) {
+    for (int o = 1; o < L; o <<= 1)
+        for (int t = 0; t < L; t += 2 * o) a[t] = a[t] + a[t + o];
+    return a[0];
+}
+template <typename T> inline V3<T> combine_lanes(V3<T>* a, int L) {
+    for (int o = 1; o < L; o <<= 1)
+        for (int t = 0; t < L; t += 2 * o) a[t] = add(a[t], a[t + o]);
+    return a[0];
+}
 // glm compute_dot and the reference Vec3 dot: (x*x + y*y) + z*z
 template <typename T> inline T dot_ref(const V3<T>& a, const V3<T>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 // product: fma(z,z, fma(y,y, x*x))
@@ -495,25 +512,39 @@ public:
 
     const int* nb(int i) const { return &nbr[(size_t)i * p.max_nbr]; }
 
+    // pair lanes of the product arithmetic (reference arithmetic: one sequential sum)
+    int lanes() const {
+        if (!(p.arith == 1 && !is_double) || p.lanes <= 1) return 1;
+        return std::min(p.lanes, kMaxLanes);
+    }
+
     void compute_lambda() {
         // calculateLambda cu:156-180; CPU src/solver.cpp:78-95
+        const int L = lanes();
         for (int i = 0; i < n; ++i) {
-            T r = 0, gm = 0;
-            V3<T> gs{0, 0, 0};
-            for (int q = 0; q < ncnt[i]; ++q) {
-                const int j = nb(i)[q];
-                const V3<T> d = sub(x[i], x[j]);
-                r += W6(d);
-                const V3<T> g = gradW(d);
-                gs = {gs.x + g.x, gs.y + g.y, gs.z + g.z};
-                if (p.arith == 1 && !is_double) {
-                    gm = std::fma(g.x, g.x, gm);
-                    gm = std::fma(g.y, g.y, gm);
-                    gm = std::fma(g.z, g.z, gm);
-                } else {
-                    gm += dot_ref(g, g);
+            T rl[kMaxLanes], gml[kMaxLanes];
+            V3<T> gsl[kMaxLanes];
+            for (int t = 0; t < L; ++t) {
+                T r = 0, gm = 0;
+                V3<T> gs{0, 0, 0};
+                for (int q = t; q < ncnt[i]; q += L) {
+                    const int j = nb(i)[q];
+                    const V3<T> d = sub(x[i], x[j]);
+                    r += W6(d);
+                    const V3<T> g = gradW(d);
+                    gs = {gs.x + g.x, gs.y + g.y, gs.z + g.z};
+                    if (p.arith == 1 && !is_double) {
+                        gm = std::fma(g.x, g.x, gm);
+                        gm = std::fma(g.y, g.y, gm);
+                        gm = std::fma(g.z, g.z, gm);
+                    } else {
+                        gm += dot_ref(g, g);
+                    }
                 }
+                rl[t] = r; gml[t] = gm; gsl[t] = gs;
             }
+            T r = combine_lanes(rl, L), gm = combine_lanes(gml, L);
+            V3<T> gs = combine_lanes(gsl, L);
             if (p.flags & ORACLE_WALL_DENSITY) {
                 V3<T> gw;
                 r = r + wall_term(x[i], gw);
@@ -540,24 +571,30 @@ public:
 
     void compute_dp() {
         // calculateOffset cu:182-199; CPU src/solver.cpp:97-108
+        const int L = lanes();
         for (int i = 0; i < n; ++i) {
-            V3<T> a{0, 0, 0};
+            V3<T> al[kMaxLanes];
             T mag = 0;
-            for (int q = 0; q < ncnt[i]; ++q) {
-                const int j = nb(i)[q];
-                const V3<T> d = sub(x[i], x[j]);
-                const T w = W6(d);
-                const V3<T> g = gradW(d);
-                const T s = (lambda[i] + lambda[j]) + scorr(w);
-                if (p.arith == 1 && !is_double) {
-                    a.x = std::fma(s, g.x, a.x);
-                    a.y = std::fma(s, g.y, a.y);
-                    a.z = std::fma(s, g.z, a.z);
-                } else {
-                    a = {a.x + s * g.x, a.y + s * g.y, a.z + s * g.z};
+            for (int t = 0; t < L; ++t) {
+                V3<T> a{0, 0, 0};
+                for (int q = t; q < ncnt[i]; q += L) {
+                    const int j = nb(i)[q];
+                    const V3<T> d = sub(x[i], x[j]);
+                    const T w = W6(d);
+                    const V3<T> g = gradW(d);
+                    const T s = (lambda[i] + lambda[j]) + scorr(w);
+                    if (p.arith == 1 && !is_double) {
+                        a.x = std::fma(s, g.x, a.x);
+                        a.y = std::fma(s, g.y, a.y);
+                        a.z = std::fma(s, g.z, a.z);
+                    } else {
+                        a = {a.x + s * g.x, a.y + s * g.y, a.z + s * g.z};
+                    }
+                    mag += std::fabs(s) * (std::fabs(g.x) + std::fabs(g.y) + std::fabs(g.z));
                 }
-                mag += std::fabs(s) * (std::fabs(g.x) + std::fabs(g.y) + std::fabs(g.z));
+                al[t] = a;
             }
+            V3<T> a = combine_lanes(al, L);
             if (p.flags & ORACLE_WALL_DENSITY) {
                 V3<T> gw;
                 wall_term(x[i], gw);
@@ -589,46 +626,57 @@ public:
                 v[i] = {(x[i].x - xold[i].x) * invDt, (x[i].y - xold[i].y) * invDt, (x[i].z - xold[i].z) * invDt};
         }
         const bool pa = p.arith == 1 && !is_double;
+        const int L = lanes();
         for (int i = 0; i < n; ++i) {
-            V3<T> w{0, 0, 0};
-            for (int q = 0; q < ncnt[i]; ++q) {
-                const int j = nb(i)[q];
-                // GPU: (v_j - v_i) x gradW ; CPU: (v_i - v_j) x gradW
-                const V3<T> vij = p.formulation == 0 ? sub(v[j], v[i]) : sub(v[i], v[j]);
-                const V3<T> c = cross(vij, gradW(sub(x[i], x[j])));
-                w = {w.x + c.x, w.y + c.y, w.z + c.z};
+            V3<T> wl[kMaxLanes];
+            for (int t = 0; t < L; ++t) {
+                V3<T> w{0, 0, 0};
+                for (int q = t; q < ncnt[i]; q += L) {
+                    const int j = nb(i)[q];
+                    // GPU: (v_j - v_i) x gradW ; CPU: (v_i - v_j) x gradW
+                    const V3<T> vij = p.formulation == 0 ? sub(v[j], v[i]) : sub(v[i], v[j]);
+                    const V3<T> c = cross(vij, gradW(sub(x[i], x[j])));
+                    w = {w.x + c.x, w.y + c.y, w.z + c.z};
+                }
+                wl[t] = w;
             }
-            curl[i] = w;
+            curl[i] = combine_lanes(wl, L);
         }
         for (int i = 0; i < n; ++i) {
-            V3<T> pv{0, 0, 0}, eta{0, 0, 0};
-            for (int q = 0; q < ncnt[i]; ++q) {
-                const int j = nb(i)[q];
-                const V3<T> d = sub(x[i], x[j]);
-                const T w = W6(d);
-                if (pa) {
-                    const V3<T> vji = sub(v[j], v[i]);
-                    pv.x = std::fma(vji.x, w, pv.x);
-                    pv.y = std::fma(vji.y, w, pv.y);
-                    pv.z = std::fma(vji.z, w, pv.z);
-                    const T wl = std::sqrt(dot_fma(curl[j], curl[j]));
-                    const V3<T> g = gradW(d);
-                    eta.x = std::fma(wl, g.x, eta.x);
-                    eta.y = std::fma(wl, g.y, eta.y);
-                    eta.z = std::fma(wl, g.z, eta.z);
-                } else {
-                    const V3<T> vij = sub(v[i], v[j]);
-                    pv = {pv.x - vij.x * w, pv.y - vij.y * w, pv.z - vij.z * w};
-                    if (p.formulation == 0) {
-                        const T wl = std::sqrt(dot_ref(curl[j], curl[j]));
+            V3<T> pvl[kMaxLanes], etal[kMaxLanes];
+            for (int t = 0; t < L; ++t) {
+                V3<T> pv{0, 0, 0}, eta{0, 0, 0};
+                for (int q = t; q < ncnt[i]; q += L) {
+                    const int j = nb(i)[q];
+                    const V3<T> d = sub(x[i], x[j]);
+                    const T w = W6(d);
+                    if (pa) {
+                        const V3<T> vji = sub(v[j], v[i]);
+                        pv.x = std::fma(vji.x, w, pv.x);
+                        pv.y = std::fma(vji.y, w, pv.y);
+                        pv.z = std::fma(vji.z, w, pv.z);
+                        const T wl = std::sqrt(dot_fma(curl[j], curl[j]));
                         const V3<T> g = gradW(d);
-                        eta = {eta.x + wl * g.x, eta.y + wl * g.y, eta.z + wl * g.z};
+                        eta.x = std::fma(wl, g.x, eta.x);
+                        eta.y = std::fma(wl, g.y, eta.y);
+                        eta.z = std::fma(wl, g.z, eta.z);
                     } else {
-                        const T s = std::sqrt(dot_ref(curl[j], curl[j])) * w;  // glm vec3 += scalar
-                        eta = {eta.x + s, eta.y + s, eta.z + s};
+                        const V3<T> vij = sub(v[i], v[j]);
+                        pv = {pv.x - vij.x * w, pv.y - vij.y * w, pv.z - vij.z * w};
+                        if (p.formulation == 0) {
+                            const T wl = std::sqrt(dot_ref(curl[j], curl[j]));
+                            const V3<T> g = gradW(d);
+                            eta = {eta.x + wl * g.x, eta.y + wl * g.y, eta.z + wl * g.z};
+                        } else {
+                            const T s = std::sqrt(dot_ref(curl[j], curl[j])) * w;  // glm vec3 += scalar
+                            eta = {eta.x + s, eta.y + s, eta.z + s};
+                        }
                     }
                 }
+                pvl[t] = pv; etal[t] = eta;
             }
+            const V3<T> pv = combine_lanes(pvl, L);
+            V3<T> eta = combine_lanes(etal, L);
             const T el = std::sqrt(pa ? dot_fma(eta, eta) : dot_ref(eta, eta));
             if (p.formulation == 0) {
                 if ((double)el > 1e-3) eta = {eta.x / el, eta.y / el, eta.z / el};

@@ -1,9 +1,12 @@
-"""Autotuner for the neighbour passes: picks the threads per block and the grid
-cell size (h or h/2 with a 5x5x5 stencil) of a workload by timing each
-candidate on the GPU from the same initial state, and caches the choice.
+"""Autotuner for the neighbour passes: picks the threads per block, the pair
+lanes per particle and the grid cell size (h or h/2 with a 5x5x5 stencil) of a
+workload by timing each candidate on the GPU from the same initial state, and
+caches the choice.
 
-The candidates change only the launch shape and the neighbour-list order, not
-the neighbour sets (test_gpu_batch.py checks the sets for cells of h/2).
+The candidates change the launch shape, the neighbour-list order and the FP32
+summation order (pair lanes), never the neighbour sets (test_gpu_batch.py checks
+the sets for cells of h/2); every candidate is bit-exact with the oracle run
+with the same settings.
 """
 from __future__ import annotations
 
@@ -12,7 +15,7 @@ import math
 import os
 from typing import Optional, Sequence
 
-CANDIDATES = [(cs, bs) for cs in (1.0, 0.5) for bs in (128, 256)]
+CANDIDATES = [(cs, bs, ln) for cs in (1.0, 0.5) for bs in (128, 256) for ln in (2, 4, 8)]
 
 
 def dims_for_scale(dims: Sequence[int], cell_scale: float) -> list:
@@ -25,7 +28,12 @@ def signature(scenes, iterations: int) -> str:
     return f"scenes={len(scenes)}:n={n}:h={float(scenes[0].para.h):.6g}:it={iterations}"
 
 
-def _time_candidate(scenes, iterations, cell_scale, block, substeps, warm):
+def ext_for(tuned: dict) -> dict:
+    """Ext overrides of a tuning result (grid_dims excluded: they are per scene)."""
+    return {"cell_scale": tuned["cell_scale"], "block_size": tuned["block_size"], "pair_lanes": tuned["pair_lanes"]}
+
+
+def _time_candidate(scenes, iterations, cell_scale, block, lanes, substeps, warm):
     import torch
 
     from . import scenes as S
@@ -34,13 +42,14 @@ def _time_candidate(scenes, iterations, cell_scale, block, substeps, warm):
     if len(scs) == 1:
         sc = scs[0]
         dims = dims_for_scale(sc.ext_overrides["grid_dims"], cell_scale)
-        s = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(grid_dims=dims, cell_scale=cell_scale, block_size=block))
+        s = Solver(sc.para, sc.grid_space, sc.boundary,
+                   sc.ext(grid_dims=dims, cell_scale=cell_scale, block_size=block, pair_lanes=lanes))
         s.upload(sc.pos, sc.vel)
     else:
         para, descs, ov, pos, vel = S.batch_inputs(scs, iterations=iterations)
         for d in descs:
             d["grid_dims"] = dims_for_scale(d["grid_dims"], cell_scale)
-        ov.update(cell_scale=cell_scale, block_size=block)
+        ov.update(cell_scale=cell_scale, block_size=block, pair_lanes=lanes)
         s = BatchSolver(para, descs, S.default_ext(**ov))
         s.upload(pos, vel)
     st = torch.cuda.current_stream()
@@ -57,8 +66,8 @@ def _time_candidate(scenes, iterations, cell_scale, block, substeps, warm):
 
 def tune(scenes, iterations: int = 4, substeps: int = 6, warm: int = 2, candidates=None,
          cache_path: Optional[str] = None) -> dict:
-    """Times every (cell_scale, block_size) candidate and returns the fastest:
-    {"cell_scale", "block_size", "ms_per_substep", "table"}."""
+    """Times every (cell_scale, block_size, pair_lanes) candidate and returns the
+    fastest: {"cell_scale", "block_size", "pair_lanes", "ms_per_substep", "table"}."""
     key = signature(scenes, iterations)
     if cache_path and os.path.exists(cache_path):
         with open(cache_path) as f:
@@ -66,9 +75,9 @@ def tune(scenes, iterations: int = 4, substeps: int = 6, warm: int = 2, candidat
         if key in cache:
             return cache[key]
     table = []
-    for cs, bs in candidates or CANDIDATES:
-        table.append({"cell_scale": cs, "block_size": bs,
-                      "ms_per_substep": _time_candidate(scenes, iterations, cs, bs, substeps, warm)})
+    for cs, bs, ln in candidates or CANDIDATES:
+        table.append({"cell_scale": cs, "block_size": bs, "pair_lanes": ln,
+                      "ms_per_substep": _time_candidate(scenes, iterations, cs, bs, ln, substeps, warm)})
     best = min(table, key=lambda r: r["ms_per_substep"])
     out = dict(best)
     out["table"] = table

@@ -164,6 +164,7 @@ KParams make_kparams(const pbf_solver& s) {
     k.radius = e.cell_scale >= 1.0f ? 1 : (int)std::ceil(1.0 / (double)e.cell_scale);
     k.n = s.n;
     k.block = e.block_size > 0 ? e.block_size : 256;
+    k.lanes = e.pair_lanes > 0 ? e.pair_lanes : 4;
     k.max_nbr = e.max_neighbors;
     k.stride = s.stride;
     k.cell_order = e.cell_order;
@@ -250,6 +251,8 @@ int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, co
         return fail(PBF_ERR_INVALID, "iterations exceeds max_iterations");
     if (!std::isfinite(e->density_tol) || e->density_tol < 0) return fail(PBF_ERR_INVALID, "density_tol must be >= 0");
     if (!std::isfinite(e->warm_clamp) || e->warm_clamp < 0) return fail(PBF_ERR_INVALID, "warm_clamp must be >= 0");
+    if (e->pair_lanes != 0 && e->pair_lanes != 1 && e->pair_lanes != 2 && e->pair_lanes != 4 && e->pair_lanes != 8)
+        return fail(PBF_ERR_INVALID, "pair_lanes must be 0, 1, 2, 4 or 8");
     return PBF_OK;
 }
 
@@ -436,6 +439,7 @@ void pbf_ext_params_default(pbf_ext_params* e) {
     e->density_tol = 0.01f;
     e->max_iterations = 16;
     e->warm_clamp = 4.0f;
+    e->pair_lanes = 4;
 }
 
 int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], const float boundary[6],

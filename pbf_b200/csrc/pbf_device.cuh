@@ -65,6 +65,7 @@ struct KParams {
     int radius;     // stencil radius in cells: ceil(1 / cell_scale)
     int n;          // particles
     int block;      // threads per block of the neighbour passes
+    int lanes;      // pair lanes per particle of the neighbour passes (1, 2, 4, 8)
     int max_nbr;    // neighbour cap (reference MAX_NEIGHBOR = 63)
     int stride;     // neighbour list stride (slot-major layout: nbr[q * stride + k])
     int cell_order; // 0 ascending, 1 descending within a cell

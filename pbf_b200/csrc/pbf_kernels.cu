@@ -18,6 +18,8 @@
 // applyVorticityAndViscosity :24-29.
 #include "pbf_kernels.h"
 
+#include <type_traits>
+
 namespace pbf {
 
 // ---------------------------------------------------------------------------
@@ -81,29 +83,36 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
                                                        int clear) {
     __shared__ int s_tile;
     __shared__ int s_warp[SCAN_THREADS / 32];
-    __shared__ int s_excl;
+    __shared__ int s_excl, s_tot;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     if (t == 0) s_tile = atomicAdd(tile_counter, 1);
     __syncthreads();
     const int tile = s_tile;
-    const long long base = (long long)tile * SCAN_TILE + (long long)t * SCAN_ITEMS;
 
+    // Warp w owns elements [tile * TILE + w * 512, +512) in 16 rounds of 32
+    // consecutive elements (one coalesced 128-byte access per round); each round
+    // is scanned across the warp and carried into the next.
+    const long long wbase = (long long)tile * SCAN_TILE + (long long)warp * (32 * SCAN_ITEMS);
     int item[SCAN_ITEMS];
-    int local = 0;
 #pragma unroll
     for (int q = 0; q < SCAN_ITEMS; ++q) {
-        const long long idx = base + q;
+        const long long idx = wbase + q * 32 + lane;
         item[q] = idx < m ? cnt[idx] : 0;
-        local += item[q];
     }
-    // block-wide exclusive scan of the per-thread totals
-    int incl = local;
+    int carry = 0;  // warp-exclusive offset of round q
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
+    for (int q = 0; q < SCAN_ITEMS; ++q) {
+        int incl = item[q];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl_q = carry + incl - item[q];
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+        item[q] = excl_q;  // now the exclusive prefix within the warp's range
     }
-    if (lane == 31) s_warp[warp] = incl;
+    if (lane == 0) s_warp[warp] = carry;  // the warp's total
     __syncthreads();
     if (warp == 0) {
         int w = lane < SCAN_THREADS / 32 ? s_warp[lane] : 0;
@@ -154,22 +163,24 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
             }
             if (lane == 0) st_release_u64(&status[tile], (2ull << 32) | (unsigned)(excl + total));
         }
-        if (lane == 0) s_excl = excl;
+        if (lane == 0) {
+            s_excl = excl;
+            s_tot = total;
+        }
     }
     __syncthreads();
-    int run = s_excl + s_warp[warp] + (incl - local);
+    const int off = s_excl + s_warp[warp];
 #pragma unroll
     for (int q = 0; q < SCAN_ITEMS; ++q) {
-        const long long idx = base + q;
+        const long long idx = wbase + q * 32 + lane;
         if (idx < m) {
-            out[idx] = run;
+            out[idx] = off + item[q];
             if (clear) cnt[idx] = 0;
         }
-        run += item[q];
     }
-    if (base <= (long long)m - 1 && (long long)m - 1 < base + SCAN_ITEMS) {
-        // the thread holding the last element writes the grand total at out[m]
-        out[m] = run;
+    if (tile == (int)(((long long)m - 1) / SCAN_TILE) && threadIdx.x == SCAN_THREADS - 1) {
+        // the last tile writes the grand total at out[m] (its inclusive prefix)
+        out[m] = s_excl + s_tot;
     }
 }
 
@@ -227,17 +238,57 @@ __global__ void __launch_bounds__(256) k_reorder(KParams p, const float4* __rest
 }
 
 // ---------------------------------------------------------------------------
+// Pair lanes. L consecutive threads of a warp (a team) share one particle. In
+// the neighbour search lane t tests candidates t, t+L, ... of each stencil row
+// and a ballot over the team appends the hits in candidate order, so the list is
+// the one a single thread builds. In the neighbour sums lane t takes list entries
+// t, t+L, t+2L, ... in order and the L partial sums are combined by an xor
+// butterfly over distances 1, 2, 4: ((p0 + p1) + (p2 + p3)) + ..., the same value
+// on every lane of the team (IEEE addition is commutative). A team shortens each
+// thread's dependent index -> position gather chain L-fold and puts L times as
+// many threads in flight.
+// ---------------------------------------------------------------------------
+template <int L> struct Team {
+    int k;          // particle slot
+    int t;          // lane within the team
+    unsigned mask;  // the team's lanes within the warp
+};
+
+// blockDim.x is a multiple of 32, so a team never straddles a warp
+template <int L> __device__ __forceinline__ Team<L> team_of() {
+    Team<L> m;
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    m.k = (int)(g / L);
+    m.t = (int)(threadIdx.x & (L - 1));
+    const int lane = threadIdx.x & 31;
+    m.mask = L >= 32 ? 0xffffffffu : (((1u << L) - 1u) << (lane & ~(L - 1)));
+    return m;
+}
+
+template <int L> __device__ __forceinline__ float team_sum(float v, unsigned mask) {
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
+template <int L> __device__ __forceinline__ f3 team_sum3(f3 v, unsigned mask) {
+    return {team_sum<L>(v.x, mask), team_sum<L>(v.y, mask), team_sum<L>(v.z, mask)};
+}
+
+// ---------------------------------------------------------------------------
 // a7: 27-cell neighbour search (a (2R+1)^3 stencil when cells are smaller than
 // h). The stencil is visited dz-major, dy, then the dx cells of a row, which are
 // one contiguous slot range because keys are x-fastest; within a cell, slot
 // order. For R = 1 this is the reference order (buildNeighborhood cu:133-136)
 // applied to the sorted slots.
 // ---------------------------------------------------------------------------
+template <int L>
 __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __restrict__ x,
                                                    const int* __restrict__ cell_start, int* __restrict__ nbr,
                                                    int* __restrict__ ncnt) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.n) return;
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
     const SceneView sc = scene_of(p, k);
     const f3 xk = make3(x[k]);
     int d[3];
@@ -247,6 +298,7 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
     const int x0 = max(d[0] - R, 0), x1 = min(d[0] + R, nx - 1);
     int c = 0;
     const int cap = p.max_nbr;
+    const unsigned below = (1u << (threadIdx.x & 31)) - 1u;  // lanes of the warp below this one
     if (x0 <= x1) {
         for (int dz = -R; dz <= R && c < cap; ++dz) {
             const int z = d[2] + dz;
@@ -256,18 +308,29 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
                 if (y < 0 || y >= ny) continue;
                 const int row = sc.cell_base + y * nx + z * nx * ny;
                 const int s = cell_start[row + x0], e = cell_start[row + x1 + 1];
-                for (int j = s; j < e && c < cap; ++j) {
-                    if (j == k) continue;
-                    const f3 r = sub3(xk, make3(x[j]));
-                    if (dot_fma(r, r) <= p.h2) {
-                        nbr[(size_t)c * p.stride + k] = j;
-                        ++c;
+                for (int j0 = s; j0 < e && c < cap; j0 += L) {
+                    const int j = j0 + tm.t;
+                    bool hit = false;
+                    if (j < e && j != k) {
+                        const f3 r = sub3(xk, make3(x[j]));
+                        hit = dot_fma(r, r) <= p.h2;
+                    }
+                    if (L == 1) {
+                        if (hit) {
+                            nbr[(size_t)c * p.stride + k] = j;
+                            ++c;
+                        }
+                    } else {
+                        const unsigned b = __ballot_sync(tm.mask, hit) & tm.mask;
+                        const int at = c + __popc(b & below);
+                        if (hit && at < cap) nbr[(size_t)at * p.stride + k] = j;
+                        c = min(c + __popc(b), cap);
                     }
                 }
             }
         }
     }
-    ncnt[k] = c;
+    if (tm.t == 0) ncnt[k] = c;
 }
 
 // ---------------------------------------------------------------------------
@@ -278,17 +341,22 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
 // requests in flight instead of one dependent index->position chain per pair.
 constexpr int NB = 4;
 
+// Entries q0, q0 + L, ..., q0 + (B-1) L of slot k's list (slot k itself past the end).
+template <int L, int B>
 __device__ __forceinline__ void load_idx(const KParams& p, const int* __restrict__ nbr, int k, int q0, int cnt,
-                                         int (&jj)[NB]) {
+                                         int (&jj)[B]) {
 #pragma unroll
-    for (int u = 0; u < NB; ++u) jj[u] = (q0 + u < cnt) ? nbr[(size_t)(q0 + u) * p.stride + k] : k;
+    for (int u = 0; u < B; ++u) {
+        const int q = q0 + u * L;
+        jj[u] = q < cnt ? nbr[(size_t)q * p.stride + k] : k;
+    }
 }
 
-template <typename V>
+template <int L, typename V>
 __device__ __forceinline__ void gather_batch(const KParams& p, const int* __restrict__ nbr, const V* __restrict__ src,
                                              int k, int q0, int cnt, V (&out)[NB]) {
     int jj[NB];
-    load_idx(p, nbr, k, q0, cnt, jj);
+    load_idx<L, NB>(p, nbr, k, q0, cnt, jj);
 #pragma unroll
     for (int u = 0; u < NB; ++u) out[u] = src[jj[u]];
 }
@@ -316,27 +384,28 @@ __device__ __forceinline__ void block_error_reduce(float e, unsigned long long* 
     }
 }
 
-template <bool DEBUG>
+template <bool DEBUG, int L>
 // 6 resident blocks per SM: 40 registers without spills (7 spills)
 __global__ void __launch_bounds__(256, 6) k_lambda(KParams p, const float4* __restrict__ x, const int* __restrict__ nbr,
                                                 const int* __restrict__ ncnt, float4* __restrict__ xl,
                                                 float* __restrict__ rho_out, IterCtl ctl) {
     if (ctl.done && *ctl.done) return;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
     float err = 0.0f;
     if (k < p.n) {
         const f3 xk = make3(x[k]);
         const int cnt = ncnt[k];
         float rho = 0.0f, gm = 0.0f;
         f3 gs = {0.0f, 0.0f, 0.0f};
-        // batches of NB neighbours: all index loads, then all position loads, then
-        // the pairs in list order (the summation order does not change)
-        for (int q0 = 0; q0 < cnt; q0 += NB) {
+        // batches of NB of this lane's entries: all index loads, then all position
+        // loads, then the pairs in list order
+        for (int q0 = tm.t; q0 < cnt; q0 += L * NB) {
             float4 xj[NB];
-            gather_batch(p, nbr, x, k, q0, cnt, xj);
+            gather_batch<L>(p, nbr, x, k, q0, cnt, xj);
 #pragma unroll
             for (int u = 0; u < NB; ++u) {
-                if (q0 + u >= cnt) break;
+                if (q0 + u * L >= cnt) break;
                 const f3 r = sub3(xk, make3(xj[u]));
                 const float r2 = dot_fma(r, r);
                 rho = rho + w_poly6(p, r2);
@@ -347,23 +416,28 @@ __global__ void __launch_bounds__(256, 6) k_lambda(KParams p, const float4* __re
                 gm = __fmaf_rn(g.z, g.z, gm);
             }
         }
-        // one-sided error of the fluid density at these positions (no wall term)
-        err = fmaxf(__fdiv_rn(rho, p.rho0) - 1.0f, 0.0f);
-        if (p.flags & FLAG_WALL_DENSITY) {
-            f3 gw;
-            rho = rho + wall_term(p, scene_of(p, k), xk, gw);
-            gs = {gs.x + gw.x, gs.y + gw.y, gs.z + gw.z};
+        rho = team_sum<L>(rho, tm.mask);
+        gm = team_sum<L>(gm, tm.mask);
+        gs = team_sum3<L>(gs, tm.mask);
+        if (tm.t == 0) {
+            // one-sided error of the fluid density at these positions (no wall term)
+            err = fmaxf(__fdiv_rn(rho, p.rho0) - 1.0f, 0.0f);
+            if (p.flags & FLAG_WALL_DENSITY) {
+                f3 gw;
+                rho = rho + wall_term(p, scene_of(p, k), xk, gw);
+                gs = {gs.x + gw.x, gs.y + gw.y, gs.z + gw.z};
+            }
+            float C = __fdiv_rn(rho, p.rho0) - 1.0f;
+            if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
+            gm = __fmaf_rn(gs.x, gs.x, gm);
+            gm = __fmaf_rn(gs.y, gs.y, gm);
+            gm = __fmaf_rn(gs.z, gs.z, gm);
+            gm = __fdiv_rn(gm, p.rho0sq);
+            const float lam = __fdiv_rn(-C, gm + p.eps);
+            xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
+            if (ctl.lam_acc) ctl.lam_acc[k] += lam;
+            if (DEBUG) rho_out[k] = rho;
         }
-        float C = __fdiv_rn(rho, p.rho0) - 1.0f;
-        if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
-        gm = __fmaf_rn(gs.x, gs.x, gm);
-        gm = __fmaf_rn(gs.y, gs.y, gm);
-        gm = __fmaf_rn(gs.z, gs.z, gm);
-        gm = __fdiv_rn(gm, p.rho0sq);
-        const float lam = __fdiv_rn(-C, gm + p.eps);
-        xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
-        if (ctl.lam_acc) ctl.lam_acc[k] += lam;
-        if (DEBUG) rho_out[k] = rho;
     }
     if (ctl.max_bits) block_error_reduce(err, ctl.max_bits, ctl.sum);
 }
@@ -381,22 +455,23 @@ __global__ void __launch_bounds__(256, 6) k_lambda(KParams p, const float4* __re
 //        fraction non-empty, maximum
 // lam_acc starts the substep's total lambda at this pass's lambda.
 // ---------------------------------------------------------------------------
+template <int L>
 __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __restrict__ x,
                                                   const float4* __restrict__ v, const int* __restrict__ nbr,
                                                   const int* __restrict__ ncnt, const int* __restrict__ cell_start,
                                                   const float* __restrict__ lam_prev, float4* __restrict__ xl,
                                                   float* __restrict__ feat, float* __restrict__ lam_acc) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.n) return;
-    const SceneView sc = scene_of(p, k);
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
     const f3 xk = make3(x[k]);
     const f3 vk = make3(v[k]);
     const int cnt = ncnt[k];
     float rho = 0.0f, gm = 0.0f, div = 0.0f;
     f3 gs = {0.0f, 0.0f, 0.0f};
-    for (int q0 = 0; q0 < cnt; q0 += NB) {
+    for (int q0 = tm.t; q0 < cnt; q0 += L * NB) {
         int jj[NB];
-        load_idx(p, nbr, k, q0, cnt, jj);
+        load_idx<L, NB>(p, nbr, k, q0, cnt, jj);
         float4 xj[NB], vj[NB];
 #pragma unroll
         for (int u = 0; u < NB; ++u) {
@@ -405,7 +480,7 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
         }
 #pragma unroll
         for (int u = 0; u < NB; ++u) {
-            if (q0 + u >= cnt) break;
+            if (q0 + u * L >= cnt) break;
             const f3 r = sub3(xk, make3(xj[u]));
             const float r2 = dot_fma(r, r);
             rho = rho + w_poly6(p, r2);
@@ -420,6 +495,12 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
             div = __fmaf_rn(vji.z, g.z, div);
         }
     }
+    rho = team_sum<L>(rho, tm.mask);
+    gm = team_sum<L>(gm, tm.mask);
+    gs = team_sum3<L>(gs, tm.mask);
+    div = team_sum<L>(div, tm.mask);
+    if (tm.t != 0) return;
+    const SceneView sc = scene_of(p, k);
     const float rho_fluid = rho;
     if (p.flags & FLAG_WALL_DENSITY) {
         f3 gw;
@@ -507,7 +588,7 @@ __global__ void k_count_fallback(const int* __restrict__ iters, int first, int c
 // and on the last iteration v = (x - x_old) / dt
 // (calculateOffset cu:182-199, updatePosition cu:15-22)
 // ---------------------------------------------------------------------------
-template <bool DEBUG>
+template <bool DEBUG, int L>
 __global__ void __launch_bounds__(256, 6) k_dp(KParams p, const float4* __restrict__ xl, const int* __restrict__ nbr,
                                             const int* __restrict__ ncnt, const float4* __restrict__ xold,
                                             float4* __restrict__ xout, float4* __restrict__ vout,
@@ -525,19 +606,20 @@ __global__ void __launch_bounds__(256, 6) k_dp(KParams p, const float4* __restri
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ctl.iters, 1);
     }
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.n) return;
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
     const float4 xk4 = xl[k];
     const f3 xk = make3(xk4);
     const float lk = xk4.w;
     const int cnt = ncnt[k];
     f3 a = {0.0f, 0.0f, 0.0f};
-    for (int q0 = 0; q0 < cnt; q0 += NB) {
+    for (int q0 = tm.t; q0 < cnt; q0 += L * NB) {
         float4 xj[NB];
-        gather_batch(p, nbr, xl, k, q0, cnt, xj);
+        gather_batch<L>(p, nbr, xl, k, q0, cnt, xj);
 #pragma unroll
         for (int u = 0; u < NB; ++u) {
-            if (q0 + u >= cnt) break;
+            if (q0 + u * L >= cnt) break;
             const float4 xj4 = xj[u];
             const f3 r = sub3(xk, make3(xj4));
             const float r2 = dot_fma(r, r);
@@ -549,6 +631,8 @@ __global__ void __launch_bounds__(256, 6) k_dp(KParams p, const float4* __restri
             a.z = __fmaf_rn(s, g.z, a.z);
         }
     }
+    a = team_sum3<L>(a, tm.mask);
+    if (tm.t != 0) return;
     if (p.flags & FLAG_WALL_DENSITY) {
         f3 gw;
         wall_term(p, scene_of(p, k), xk, gw);
@@ -580,18 +664,20 @@ __global__ void __launch_bounds__(256) k_velocity(KParams p, const float4* __res
 // ---------------------------------------------------------------------------
 // a12: vorticity (calculateCurl cu:201-215): w_i = sum (v_j - v_i) x gradW(x_i - x_j)
 // ---------------------------------------------------------------------------
+template <int L>
 __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
                                               const int* __restrict__ nbr, const int* __restrict__ ncnt,
                                               float4* __restrict__ omega) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.n) return;
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
     const f3 xk = make3(x[k]);
     const f3 vk = make3(v[k]);
     const int cnt = ncnt[k];
     f3 w = {0.0f, 0.0f, 0.0f};
-    for (int q0 = 0; q0 < cnt; q0 += NB) {
+    for (int q0 = tm.t; q0 < cnt; q0 += L * NB) {
         int jj[NB];
-        load_idx(p, nbr, k, q0, cnt, jj);
+        load_idx<L, NB>(p, nbr, k, q0, cnt, jj);
         float4 xj[NB], vj[NB];
 #pragma unroll
         for (int u = 0; u < NB; ++u) {
@@ -600,45 +686,48 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
         }
 #pragma unroll
         for (int u = 0; u < NB; ++u) {
-            if (q0 + u >= cnt) break;
+            if (q0 + u * L >= cnt) break;
             const f3 r = sub3(xk, make3(xj[u]));
             const f3 g = grad_spiky(p, r, dot_fma(r, r));
             const f3 c = cross3(sub3(make3(vj[u]), vk), g);
             w = {w.x + c.x, w.y + c.y, w.z + c.z};
         }
     }
-    omega[k] = make_float4(w.x, w.y, w.z, 0.0f);
+    w = team_sum3<L>(w, tm.mask);
+    if (tm.t == 0) omega[k] = make_float4(w.x, w.y, w.z, 0.0f);
 }
 
 // ---------------------------------------------------------------------------
 // a13: vorticity confinement and XSPH, applied to v
 // (calculateVorticityAndViscosity cu:217-239, applyVorticityAndViscosity cu:24-29)
 // ---------------------------------------------------------------------------
-template <bool DEBUG>
+template <bool DEBUG, int L>
 __global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
                                               const float4* __restrict__ omega, const int* __restrict__ nbr,
                                               const int* __restrict__ ncnt, float4* __restrict__ vout,
                                               const int* __restrict__ perm_in, int* __restrict__ perm_out,
                                               float4* __restrict__ vort_out, float4* __restrict__ visc_out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= p.n) return;
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
     const f3 xk = make3(x[k]);
     const f3 vk = make3(v[k]);
     const int cnt = ncnt[k];
     f3 pv = {0.0f, 0.0f, 0.0f}, eta = {0.0f, 0.0f, 0.0f};
-    for (int q0 = 0; q0 < cnt; q0 += NB) {
-        int jj[NB];
-        load_idx(p, nbr, k, q0, cnt, jj);
-        float4 xj[NB], vj[NB], oj4[NB];
+    constexpr int NBV = 2;  // entries per batch: three 16-byte gathers each
+    for (int q0 = tm.t; q0 < cnt; q0 += L * NBV) {
+        int jj[NBV];
+        load_idx<L, NBV>(p, nbr, k, q0, cnt, jj);
+        float4 xj[NBV], vj[NBV], oj4[NBV];
 #pragma unroll
-        for (int u = 0; u < NB; ++u) {
+        for (int u = 0; u < NBV; ++u) {
             xj[u] = x[jj[u]];
             vj[u] = v[jj[u]];
             oj4[u] = omega[jj[u]];
         }
 #pragma unroll
-        for (int u = 0; u < NB; ++u) {
-            if (q0 + u >= cnt) break;
+        for (int u = 0; u < NBV; ++u) {
+            if (q0 + u * L >= cnt) break;
             const f3 r = sub3(xk, make3(xj[u]));
             const float r2 = dot_fma(r, r);
             const float w = w_poly6(p, r2);
@@ -654,6 +743,9 @@ __global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restric
             eta.z = __fmaf_rn(wl, g.z, eta.z);
         }
     }
+    pv = team_sum3<L>(pv, tm.mask);
+    eta = team_sum3<L>(eta, tm.mask);
+    if (tm.t != 0) return;
     const float el = __fsqrt_rn(dot_fma(eta, eta));
     if ((double)el > 1e-3) eta = {__fdiv_rn(eta.x, el), __fdiv_rn(eta.y, el), __fdiv_rn(eta.z, el)};
     const f3 cr = cross3(eta, make3(omega[k]));
@@ -757,6 +849,18 @@ __global__ void k_copy4(int n, const float4* __restrict__ a, float4* __restrict_
 // launchers
 // ---------------------------------------------------------------------------
 static inline int blocks_for(int n, int bs) { return (n + bs - 1) / bs; }
+// blocks for n particles with L threads each
+static inline int team_blocks(int n, int L, int bs) { return (int)(((long long)n * L + bs - 1) / bs); }
+
+// Calls f with the pair-lane count as a compile-time constant.
+template <typename F> void with_lanes(int lanes, F&& f) {
+    switch (lanes) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        default: f(std::integral_constant<int, 4>{}); break;
+    }
+}
 
 void launch_hash(const KParams& p, bool predict_on, const float4* x, const float4* v, int* cell, int* ticket, int* cnt,
                  int* err, cudaStream_t st) {
@@ -804,28 +908,40 @@ void launch_reorder(const KParams& p, bool predict_on, const float4* x, const fl
 }
 
 void launch_neighbors(const KParams& p, const float4* x, const int* cell_start, int* nbr, int* ncnt, cudaStream_t st) {
-    k_neighbors<<<blocks_for(p.n, p.block), p.block, 0, st>>>(p, x, cell_start, nbr, ncnt);
+    with_lanes(p.lanes, [&](auto lc) {
+        constexpr int L = decltype(lc)::value;
+        k_neighbors<L><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, cell_start, nbr, ncnt);
+    });
 }
 
 void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr, const int* ncnt, float4* xl,
                    float* rho, const IterCtl& ctl, cudaStream_t st) {
-    const int b = blocks_for(p.n, p.block);
-    if (debug) k_lambda<true><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
-    else k_lambda<false><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+    with_lanes(p.lanes, [&](auto lc) {
+        constexpr int L = decltype(lc)::value;
+        const int b = team_blocks(p.n, L, p.block);
+        if (debug) k_lambda<true, L><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+        else k_lambda<false, L><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+    });
 }
 
 void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, const int* ncnt, const float4* xold,
                float4* xout, float4* vout, float4* dp, const IterCtl& ctl, cudaStream_t st) {
-    const int b = blocks_for(p.n, p.block);
-    if (debug) k_dp<true><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
-    else k_dp<false><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+    with_lanes(p.lanes, [&](auto lc) {
+        constexpr int L = decltype(lc)::value;
+        const int b = team_blocks(p.n, L, p.block);
+        if (debug) k_dp<true, L><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+        else k_dp<false, L><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+    });
 }
 
 void launch_features(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
                      const int* cell_start, const float* lam_prev, float4* xl, float* feat, float* lam_acc,
                      cudaStream_t st) {
-    k_features<<<blocks_for(p.n, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, cell_start, lam_prev, xl, feat,
-                                                              lam_acc);
+    with_lanes(p.lanes, [&](auto lc) {
+        constexpr int L = decltype(lc)::value;
+        k_features<L><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, cell_start, lam_prev,
+                                                                         xl, feat, lam_acc);
+    });
 }
 
 void launch_gather_rows(const int* slots, int count, int n, const float* feat, const float* lam_acc, float* out_feat,
@@ -845,15 +961,23 @@ void launch_velocity(const KParams& p, const float4* x, const float4* xold, floa
 
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
                  cudaStream_t st) {
-    k_curl<<<blocks_for(p.n, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, omega);
+    with_lanes(p.lanes, [&](auto lc) {
+        constexpr int L = decltype(lc)::value;
+        k_curl<L><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, omega);
+    });
 }
 
 void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v, const float4* omega, const int* nbr,
                  const int* ncnt, float4* vout, const int* perm_in, int* perm_out, float4* vort, float4* visc,
                  cudaStream_t st) {
-    const int b = blocks_for(p.n, p.block);
-    if (debug) k_vort<true><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, vout, perm_in, perm_out, vort, visc);
-    else k_vort<false><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, vout, perm_in, perm_out, vort, visc);
+    with_lanes(p.lanes, [&](auto lc) {
+        constexpr int L = decltype(lc)::value;
+        const int b = team_blocks(p.n, L, p.block);
+        if (debug)
+            k_vort<true, L><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, vout, perm_in, perm_out, vort, visc);
+        else
+            k_vort<false, L><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, vout, perm_in, perm_out, vort, visc);
+    });
 }
 
 void launch_density_error(const KParams& p, const float4* x, const int* nbr, const int* ncnt,

@@ -67,6 +67,20 @@ def test_single_substep_bitexact(block, iters):
     assert_substep_bitexact(s, orc)
 
 
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8])
+@pytest.mark.parametrize("cell_scale", [1.0, 0.5])
+def test_pair_lanes_bitexact(lanes, cell_scale):
+    """Every pair-lane count: the neighbour lists are the single-thread lists and
+    the lane sums follow the oracle's butterfly order bit for bit."""
+    sc = scenes.dam_break(16, (40, 20, 20), stable=True, iterations=3)
+    ext = {"pair_lanes": lanes, "cell_scale": cell_scale,
+           "grid_dims": [int(round(d / cell_scale)) for d in sc.ext_overrides["grid_dims"]]}
+    s, orc = make_pair(sc, **ext)
+    s.step(2)
+    orc.substep(2)
+    assert_substep_bitexact(s, orc)
+
+
 def test_reference_formulas_single_substep_bitexact():
     """Reference parameter values without the stable-mode departures (the
     reference formulas, which diverge within a few substeps at these values)."""

@@ -144,3 +144,22 @@ def test_oracle_product_vs_reference_arithmetic_close():
     interior = np.all((xa > np.array(sc.boundary[:3]) + 0.02) & (xa < np.array(sc.boundary[3:]) - 0.02), axis=1)
     assert interior.mean() > 0.5
     assert np.abs(xa[interior] - xb[interior]).max() <= 1e-5 * np.abs(xa).max()
+
+
+@pytest.mark.parametrize("lanes", [2, 4, 8])
+def test_oracle_pair_lane_sums_depart_only_by_rounding(lanes):
+    """Splitting a neighbour sum over pair lanes changes only the FP32 summation
+    order: against one sequential sum, lambda and positions agree to rounding."""
+    sc = scenes.dam_break(16, (40, 20, 20), stable=True)
+    base = dict(gravity=(0.0, -9.8, 0.0), dims=(40, 20, 20), formulation=0, arith=1,
+                flags=sc.ext_overrides["flags"], scorr_scale=sc.ext_overrides["scorr_scale"], iterations=4)
+    a = O.Oracle(O.params_from(sc.para, sc.grid_space, sc.boundary, lanes=1, **base), sc.pos, sc.vel)
+    b = O.Oracle(O.params_from(sc.para, sc.grid_space, sc.boundary, lanes=lanes, **base), sc.pos, sc.vel)
+    a.substep()
+    b.substep()
+    assert np.array_equal(a.get("nbr"), b.get("nbr"))
+    lam_a, lam_b = a.get("lambda"), b.get("lambda")
+    assert not np.array_equal(lam_a, lam_b)  # the order does change the rounding
+    scale = a.get("rho").max() / float(sc.para.restRho) / float(sc.para.epsilon)
+    assert np.abs(lam_a - lam_b).max() <= 1e-5 * scale
+    assert np.abs(a.get("x") - b.get("x")).max() <= 1e-5 * np.abs(a.get("x")).max()
