@@ -212,7 +212,11 @@ def run_b200(args) -> int:
     sc = scenes.config1(seed=rank, iterations=4)
     n = sc.n
     stream = torch.cuda.current_stream()
-    tuned = autotune.tune([sc], iterations=4)
+    if args.pair_lanes and args.cell_scale and args.block_size:
+        tuned = {"cell_scale": args.cell_scale, "block_size": args.block_size, "pair_lanes": args.pair_lanes,
+                 "table": "fixed on the command line"}
+    else:
+        tuned = autotune.tune([sc], iterations=4)
     ext_kw = dict(grid_dims=autotune.dims_for_scale(sc.ext_overrides["grid_dims"], tuned["cell_scale"]),
                   **autotune.ext_for(tuned))
     solver = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(**ext_kw))
@@ -474,15 +478,19 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
 def measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, weights) -> dict:
     """The 4,194,304-particle double dam break (two 128^3 blocks, sphere of radius
     20h at the centre of a 320h x 160h x 160h box) batched with 8 scenes of
-    65,536 particles: plain 4 iterations, and the learned warm start with 2
-    iterations plus the adaptive plain fallback up to 16 iterations while the
-    max density error exceeds 10 %."""
+    65,536 particles: plain with 4 iterations; then, at the max density error the
+    plain run reached (mean over its substeps) as the tolerance, the adaptive
+    plain loop and the learned warm start + adaptive plain loop (at least 2
+    corrections, at most 16)."""
     from pbf_b200 import BatchSolver, learned, multigpu, scenes
     out = {"workload": "double dam break 2 x 128^3 + sphere r=20h, box 320h x 160h x 160h, + 8 x 65,536"}
     w16, b32 = weights
-    for label, iters, kw in (("plain", 4, {}),
-                             ("learned_adaptive", 2, {"warm_start": 1, "adaptive": 1, "density_tol": 0.1,
-                                                      "max_iterations": 16})):
+    legs = [("plain", 4, {})]
+    for label, iters, kw in legs + [("plain_adaptive", 2, {"adaptive": 1, "max_iterations": 16}),
+                                    ("learned_adaptive", 2, {"warm_start": 1, "adaptive": 1,
+                                                             "max_iterations": 16})]:
+        if kw.get("adaptive"):
+            kw = dict(kw, density_tol=out["plain"]["density_error"]["max"])
         scs = scenes.config4(seed=0, iterations=iters)
         parts = multigpu.assign_scenes([x.n for x in scs], world)
         mine = [scs[i] for i in parts[rank]]
@@ -493,12 +501,15 @@ def measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, wei
             learned.install(b, w16, b32)
         b.upload(pos, vel)
         b.step(max(args.warmup, 3), stream)
+        before = b.stats()
         t, err = _timed_errors(b, args.steps, flush, stream, barrier, max_over_ranks)
         total = sum(x.n for x in scs)
         st = b.stats()
-        out[label] = {"iterations": iters, "particles": total, "value": total * args.steps / t, "unit": UNIT,
+        out[label] = {"min_iterations": iters, "particles": total, "value": total * args.steps / t, "unit": UNIT,
                       "ms_per_step": 1e3 * t / args.steps, "density_error": err,
-                      "last_iterations": st["last_iterations"], "fallbacks": st["fallbacks"]}
+                      "mean_iterations": (st["total_iterations"] - before["total_iterations"]) / args.steps}
+        if kw.get("adaptive"):
+            out[label]["density_tol"] = kw["density_tol"]
         b.close()
     return out
 
@@ -522,6 +533,10 @@ def main() -> int:
     ap.add_argument("--legs", default="all",
                     help="comma list of legs after the single-scene one: all, batched, learned, large, cpu "
                          "(main = the single-scene leg alone)")
+    ap.add_argument("--pair-lanes", type=int, default=0, help="with --cell-scale and --block-size: skip the "
+                    "autotuner of the single-scene leg and use these launch settings")
+    ap.add_argument("--cell-scale", type=float, default=0.0)
+    ap.add_argument("--block-size", type=int, default=0)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

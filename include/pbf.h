@@ -86,8 +86,8 @@ typedef struct pbf_ext_params {
     int record_features; /* 1: keep warm-start features and total lambda (training data) */
     float warm_clamp;    /* warm start: lambda0 keeps the sign of the plain lambda of its
                             pass and at most warm_clamp times its magnitude (default 4; 0: off) */
-    int pair_lanes;      /* threads sharing one particle's neighbour loop: 1, 2, 4 or 8 (default 4;
-                            0 = 4). Lane t takes list entries t, t+L, ...; lane sums are combined
+    int pair_lanes;      /* threads sharing one particle's neighbour sums: 1, 2, 4 or 8 (default 2;
+                            0 = 2). Lane t takes list entries t, t+L, ...; lane sums are combined
                             pairwise, so the value changes the FP32 summation order */
     int reserved[3];
 } pbf_ext_params;

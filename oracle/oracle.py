@@ -58,6 +58,8 @@ def olib() -> C.CDLL:
         L.oracle_destroy.argtypes = [C.c_void_p]
         L.oracle_det_sin.restype = C.c_float
         L.oracle_det_sin.argtypes = [C.c_float]
+        L.oracle_rsqrt.restype = C.c_float
+        L.oracle_rsqrt.argtypes = [C.c_float]
         L.oracle_density_error.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.POINTER(C.c_double),
                                            C.POINTER(C.c_double), C.c_void_p]
         _olib = L
@@ -66,10 +68,10 @@ def olib() -> C.CDLL:
 
 def params_from(para, grid_space, boundary, *, gravity=(0.0, -49.0, 0.0), dims=(64, 64, 64), formulation=0,
                 arith=1, cell_order=0, reorder=1, flags=0, scorr_scale=1.0, wall_jitter=None, grad_rmin=0.01,
-                max_nbr=63, sphere=(0, 0, 0, 0), cell_scale=1.0, iterations=None, lanes=4) -> OracleParams:
+                max_nbr=63, sphere=(0, 0, 0, 0), cell_scale=1.0, iterations=None, lanes=2) -> OracleParams:
     """Oracle parameters from a SolverParameter-like object and the two AABBs.
     lanes: pair lanes per particle of the product arithmetic (the library's
-    pair_lanes, default 4)."""
+    pair_lanes, default 2)."""
     p = OracleParams()
     for f in ("h", "restRho", "epsilon", "k", "n", "deltaq", "c", "dt"):
         setattr(p, f, float(getattr(para, f)))
@@ -110,7 +112,7 @@ def params_for_scene(scene, ext=None, **kw) -> OracleParams:
                        scorr_scale=ov.get("scorr_scale", 1.0), wall_jitter=ov.get("wall_jitter", 0.01),
                        grad_rmin=ov.get("grad_rmin", 0.01), max_nbr=ov.get("max_neighbors", 63),
                        sphere=ov.get("sphere", (0, 0, 0, 0)), cell_scale=ov.get("cell_scale", 1.0),
-                       cell_order=ov.get("cell_order", 0), lanes=kw.pop("lanes", ov.get("pair_lanes", 0) or 4), **kw)
+                       cell_order=ov.get("cell_order", 0), lanes=kw.pop("lanes", ov.get("pair_lanes", 0) or 2), **kw)
 
 
 class Oracle:
@@ -161,6 +163,10 @@ class Oracle:
 
 def det_sin(a: float) -> float:
     return olib().oracle_det_sin(a)
+
+
+def rsqrt(x: float) -> float:
+    return olib().oracle_rsqrt(x)
 
 
 def density_error(pos: np.ndarray, h: float, rho0: float, per_particle: bool = False):

@@ -107,6 +107,21 @@ float det_sin(float a) {
     return (float)res;
 }
 
+// product: reciprocal square root for normal x > 0 from the published bit-level
+// estimate 0x5f3759df - (bits >> 1) (C. Lomont, "Fast Inverse Square Root",
+// 2003) and three Newton steps y <- y (3/2 - (x/2) y^2), one fused multiply-add
+// each; the CUDA library evaluates the same steps (pbf_rsqrt).
+float soft_rsqrt(float x) {
+    const float hx = 0.5f * x;
+    int32_t bits;
+    std::memcpy(&bits, &x, 4);
+    bits = 0x5f3759df - (bits >> 1);
+    float y;
+    std::memcpy(&y, &bits, 4);
+    for (int i = 0; i < 3; ++i) y = y * std::fma(-hx, y * y, 1.5f);
+    return y;
+}
+
 template <typename T> struct V3 {
     T x, y, z;
 };
@@ -252,14 +267,23 @@ public:
 
     // WspikyGrad: kernels/cudaPBFSolver.cuh:105-110 (GPU), delWspiky include/solver.h:55-60 (CPU)
     V3<T> gradW(const V3<T>& r) const {
-        if (is_double || p.arith == 1) {
-            // product: one sqrt, one division, scale the vector
-            const T r2 = is_double ? dot_ref(r, r) : dot_fma(r, r);
+        if (is_double) {
+            const T r2 = dot_ref(r, r);
             const T rl = std::sqrt(r2);
             if (rl > k.h || rl < k.rmin) return {0, 0, 0};
             const T d = k.h - rl;
             const T s = ((k.spiky_c * d) * d) / rl;
             return {s * r.x, s * r.y, s * r.z};
+        }
+        if (p.arith == 1) {
+            // product: y = rsqrt(|r|^2) by soft_rsqrt, |r| = |r|^2 y, s = c (h-|r|)^2 y
+            const float r2 = (float)dot_fma(r, r);
+            const float y = soft_rsqrt(std::max(r2, 1e-30f));
+            const float rl = r2 * y;
+            if (rl > (float)k.h || rl < (float)k.rmin) return {0, 0, 0};
+            const float d = (float)k.h - rl;
+            const float s = (((float)k.spiky_c * d) * d) * y;
+            return {(T)(s * (float)r.x), (T)(s * (float)r.y), (T)(s * (float)r.z)};
         }
         const float rl = std::sqrt((float)dot_ref(r, r));
         if (rl > (float)k.h || rl < (float)k.rmin) return {0, 0, 0};
@@ -810,6 +834,7 @@ void oracle_destroy(void* hv) {
 }
 
 float oracle_det_sin(float a) { return det_sin(a); }
+float oracle_rsqrt(float x) { return soft_rsqrt(x); }
 
 // FP64 density-error oracle: rho_i = sum_{j != i, |r|<=h} W6(r) with the exact
 // poly6 constant, over every pair (no neighbour cap), from the given positions.

@@ -15,7 +15,7 @@ import math
 import os
 from typing import Optional, Sequence
 
-CANDIDATES = [(cs, bs, ln) for cs in (1.0, 0.5) for bs in (128, 256) for ln in (2, 4, 8)]
+CANDIDATES = [(cs, bs, ln) for cs in (1.0, 0.5) for bs in (128, 256) for ln in (1, 2, 4)]
 
 
 def dims_for_scale(dims: Sequence[int], cell_scale: float) -> list:

@@ -64,6 +64,7 @@ struct DevStats {
     // not reset per substep:
     int err;
     int fallback;
+    long long total_iters;  // adaptive: corrections applied since upload
 };
 
 // Profiling stages (pbf_stage_times)
@@ -164,7 +165,7 @@ KParams make_kparams(const pbf_solver& s) {
     k.radius = e.cell_scale >= 1.0f ? 1 : (int)std::ceil(1.0 / (double)e.cell_scale);
     k.n = s.n;
     k.block = e.block_size > 0 ? e.block_size : 256;
-    k.lanes = e.pair_lanes > 0 ? e.pair_lanes : 4;
+    k.lanes = e.pair_lanes > 0 ? e.pair_lanes : 2;
     k.max_nbr = e.max_neighbors;
     k.stride = s.stride;
     k.cell_order = e.cell_order;
@@ -358,7 +359,7 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
         P(ST_MEASURE, [&] {
             launch_density_error(kp, s->Px, s->nbr, s->ncnt, &ds->max_bits[max_it], &ds->sum[max_it], &ds->done, st);
         });
-        launch_count_fallback(&ds->iters, first, iters, &ds->fallback, st);
+        launch_count_fallback(&ds->iters, first, iters, &ds->fallback, &ds->total_iters, st);
         P(ST_VELOCITY, [&] { launch_velocity(kp, s->Px, s->Pxold, s->Pv, st); });
     }
     P(ST_CURL, [&] { launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, st); });
@@ -439,7 +440,7 @@ void pbf_ext_params_default(pbf_ext_params* e) {
     e->density_tol = 0.01f;
     e->max_iterations = 16;
     e->warm_clamp = 4.0f;
-    e->pair_lanes = 4;
+    e->pair_lanes = 2;
 }
 
 int pbf_create(const pbf_solver_parameter* para, const float grid_space[6], const float boundary[6],
@@ -734,7 +735,7 @@ int pbf_get_stats(pbf_solver* s, pbf_stats* out) {
     std::memcpy(&m, &h.max_bits[slot], sizeof m);
     out->max_density_error = m;
     out->mean_density_error = h.sum[slot] / (double)s->n;
-    out->total_iterations = 0;
+    out->total_iterations = s->ext.adaptive ? h.total_iters : s->substeps * (long long)s->para.iterations;
     if (h.err) return fail(PBF_ERR_DEVICE, "kernel error bits 0x%x", h.err);
     return PBF_OK;
 }

@@ -10,8 +10,8 @@
 // Formulas follow the reference CUDA kernels (kernels/cudaPBFSolver.cuh:99-181,
 // kernels/cudaPBFSolver.cu:4-239); the departures in evaluation order are:
 //   * poly6: (h^2-r^2)^3 by two multiplies instead of powf(.,3) (cuh:102)
-//   * spiky gradient: one sqrt and one division, s = c (h-r)^2 / r, then s * r
-//     instead of powf(.,2) and normalize (cuh:106-109)
+//   * spiky gradient: one reciprocal square root y = pbf_rsqrt(|r|^2), |r| = |r|^2 y,
+//     s = c (h-|r|)^2 y, then s * r, instead of powf(.,2) and normalize (cuh:106-109)
 //   * s_corr exponent: repeated multiplication for integer n in [1,8] (cuh:143)
 //   * |r|^2 and every neighbour sum use fused multiply-adds in a fixed order
 //   * the wall-jitter hash evaluates sine with pbf_det_sin (double precision)
@@ -143,12 +143,30 @@ __device__ __forceinline__ float w_poly6(const KParams& p, float r2) {
     return p.poly6_c * ((t * t) * t);
 }
 
-// WspikyGrad (cuh:105-110): zero when |r| > h or |r| < rmin, else ((c*d)*d)/|r| * r
+// 1/sqrt(x) for normal x > 0: the published bit-level first estimate
+// 0x5f3759df - (bits(x) >> 1) (C. Lomont, "Fast Inverse Square Root", 2003),
+// then three Newton steps y <- y (3/2 - (x/2) y^2), each with one fused
+// multiply-add. Within 2 ulp of the exact value (tests check it against double
+// precision); a fixed sequence of integer and IEEE float operations, so a CPU
+// evaluation of the same steps reproduces it bit for bit. It replaces an IEEE
+// square root and an IEEE division per neighbour pair.
+__device__ __forceinline__ float pbf_rsqrt(float x) {
+    const float hx = 0.5f * x;
+    float y = __int_as_float(0x5f3759df - (__float_as_int(x) >> 1));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) y = y * __fmaf_rn(-hx, y * y, 1.5f);
+    return y;
+}
+
+// WspikyGrad (cuh:105-110): zero when |r| > h or |r| < rmin, else ((c*d)*d)/|r| * r.
+// |r|^2 is clamped to 1e-30 first so that coincident particles give |r| ~ 0
+// (cut by rmin) instead of an infinite estimate.
 __device__ __forceinline__ f3 grad_spiky(const KParams& p, const f3& r, float r2) {
-    const float rl = __fsqrt_rn(r2);
+    const float y = pbf_rsqrt(fmaxf(r2, 1e-30f));
+    const float rl = r2 * y;
     if (rl > p.h || rl < p.rmin) return {0.0f, 0.0f, 0.0f};
     const float d = p.h - rl;
-    const float s = __fdiv_rn((p.spiky_c * d) * d, rl);
+    const float s = ((p.spiky_c * d) * d) * y;
     return {s * r.x, s * r.y, s * r.z};
 }
 

@@ -238,15 +238,15 @@ __global__ void __launch_bounds__(256) k_reorder(KParams p, const float4* __rest
 }
 
 // ---------------------------------------------------------------------------
-// Pair lanes. L consecutive threads of a warp (a team) share one particle. In
-// the neighbour search lane t tests candidates t, t+L, ... of each stencil row
-// and a ballot over the team appends the hits in candidate order, so the list is
-// the one a single thread builds. In the neighbour sums lane t takes list entries
-// t, t+L, t+2L, ... in order and the L partial sums are combined by an xor
-// butterfly over distances 1, 2, 4: ((p0 + p1) + (p2 + p3)) + ..., the same value
-// on every lane of the team (IEEE addition is commutative). A team shortens each
-// thread's dependent index -> position gather chain L-fold and puts L times as
-// many threads in flight.
+// Pair lanes. L consecutive threads of a warp (a team) share one particle of the
+// neighbour sums: lane t takes list entries t, t+L, t+2L, ... in order and the L
+// partial sums are combined by an xor butterfly over distances 1, 2, 4:
+// ((p0 + p1) + (p2 + p3)) + ..., the same value on every lane of the team (IEEE
+// addition is commutative). A team shortens each thread's dependent index ->
+// position gather chain L-fold and puts L times as many threads in flight, at
+// the price of the team's shuffles and of the per-particle epilogue running on
+// one lane of L. (The neighbour search stays one thread per particle: with teams
+// it issued 2.8x the instructions for the same lists.)
 // ---------------------------------------------------------------------------
 template <int L> struct Team {
     int k;          // particle slot
@@ -282,13 +282,11 @@ template <int L> __device__ __forceinline__ f3 team_sum3(f3 v, unsigned mask) {
 // order. For R = 1 this is the reference order (buildNeighborhood cu:133-136)
 // applied to the sorted slots.
 // ---------------------------------------------------------------------------
-template <int L>
 __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __restrict__ x,
                                                    const int* __restrict__ cell_start, int* __restrict__ nbr,
                                                    int* __restrict__ ncnt) {
-    const Team<L> tm = team_of<L>();
-    const int k = tm.k;
-    if (k >= p.n) return;  // uniform over the team
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= p.n) return;
     const SceneView sc = scene_of(p, k);
     const f3 xk = make3(x[k]);
     int d[3];
@@ -298,7 +296,6 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
     const int x0 = max(d[0] - R, 0), x1 = min(d[0] + R, nx - 1);
     int c = 0;
     const int cap = p.max_nbr;
-    const unsigned below = (1u << (threadIdx.x & 31)) - 1u;  // lanes of the warp below this one
     if (x0 <= x1) {
         for (int dz = -R; dz <= R && c < cap; ++dz) {
             const int z = d[2] + dz;
@@ -308,29 +305,18 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
                 if (y < 0 || y >= ny) continue;
                 const int row = sc.cell_base + y * nx + z * nx * ny;
                 const int s = cell_start[row + x0], e = cell_start[row + x1 + 1];
-                for (int j0 = s; j0 < e && c < cap; j0 += L) {
-                    const int j = j0 + tm.t;
-                    bool hit = false;
-                    if (j < e && j != k) {
-                        const f3 r = sub3(xk, make3(x[j]));
-                        hit = dot_fma(r, r) <= p.h2;
-                    }
-                    if (L == 1) {
-                        if (hit) {
-                            nbr[(size_t)c * p.stride + k] = j;
-                            ++c;
-                        }
-                    } else {
-                        const unsigned b = __ballot_sync(tm.mask, hit) & tm.mask;
-                        const int at = c + __popc(b & below);
-                        if (hit && at < cap) nbr[(size_t)at * p.stride + k] = j;
-                        c = min(c + __popc(b), cap);
+                for (int j = s; j < e && c < cap; ++j) {
+                    if (j == k) continue;
+                    const f3 r = sub3(xk, make3(x[j]));
+                    if (dot_fma(r, r) <= p.h2) {
+                        nbr[(size_t)c * p.stride + k] = j;
+                        ++c;
                     }
                 }
             }
         }
     }
-    if (tm.t == 0) ncnt[k] = c;
+    ncnt[k] = c;
 }
 
 // ---------------------------------------------------------------------------
@@ -577,10 +563,13 @@ __global__ void k_gather_rows(const int* __restrict__ slots, int count, int n, c
     out_target[i] = lam_acc[s];
 }
 
-// Counts a substep as a fallback when the adaptive loop needed more corrections
-// than the configured iteration count.
-__global__ void k_count_fallback(const int* __restrict__ iters, int first, int configured, int* __restrict__ fallback) {
-    if (first + *iters > configured) *fallback += 1;
+// Adds the substep's corrections to the running total and counts the substep as
+// a fallback when the adaptive loop needed more than the configured count.
+__global__ void k_count_fallback(const int* __restrict__ iters, int first, int configured, int* __restrict__ fallback,
+                                 long long* __restrict__ total) {
+    const int used = first + *iters;
+    if (used > configured) *fallback += 1;
+    *total += used;
 }
 
 // ---------------------------------------------------------------------------
@@ -694,7 +683,8 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
         }
     }
     w = team_sum3<L>(w, tm.mask);
-    if (tm.t == 0) omega[k] = make_float4(w.x, w.y, w.z, 0.0f);
+    // |w| in .w: the vorticity pass needs |w_j| for every pair
+    if (tm.t == 0) omega[k] = make_float4(w.x, w.y, w.z, __fsqrt_rn(dot_fma(w, w)));
 }
 
 // ---------------------------------------------------------------------------
@@ -735,8 +725,7 @@ __global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restric
             pv.x = __fmaf_rn(vji.x, w, pv.x);
             pv.y = __fmaf_rn(vji.y, w, pv.y);
             pv.z = __fmaf_rn(vji.z, w, pv.z);
-            const f3 oj = make3(oj4[u]);
-            const float wl = __fsqrt_rn(dot_fma(oj, oj));
+            const float wl = oj4[u].w;  // |w_j| (k_curl)
             const f3 g = grad_spiky(p, r, r2);
             eta.x = __fmaf_rn(wl, g.x, eta.x);
             eta.y = __fmaf_rn(wl, g.y, eta.y);
@@ -856,9 +845,9 @@ static inline int team_blocks(int n, int L, int bs) { return (int)(((long long)n
 template <typename F> void with_lanes(int lanes, F&& f) {
     switch (lanes) {
         case 1: f(std::integral_constant<int, 1>{}); break;
-        case 2: f(std::integral_constant<int, 2>{}); break;
         case 8: f(std::integral_constant<int, 8>{}); break;
-        default: f(std::integral_constant<int, 4>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        default: f(std::integral_constant<int, 2>{}); break;
     }
 }
 
@@ -908,10 +897,7 @@ void launch_reorder(const KParams& p, bool predict_on, const float4* x, const fl
 }
 
 void launch_neighbors(const KParams& p, const float4* x, const int* cell_start, int* nbr, int* ncnt, cudaStream_t st) {
-    with_lanes(p.lanes, [&](auto lc) {
-        constexpr int L = decltype(lc)::value;
-        k_neighbors<L><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, cell_start, nbr, ncnt);
-    });
+    k_neighbors<<<blocks_for(p.n, p.block), p.block, 0, st>>>(p, x, cell_start, nbr, ncnt);
 }
 
 void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr, const int* ncnt, float4* xl,
@@ -951,8 +937,9 @@ void launch_gather_rows(const int* slots, int count, int n, const float* feat, c
                                                                err);
 }
 
-void launch_count_fallback(const int* iters, int first, int configured, int* fallback, cudaStream_t st) {
-    k_count_fallback<<<1, 1, 0, st>>>(iters, first, configured, fallback);
+void launch_count_fallback(const int* iters, int first, int configured, int* fallback, long long* total,
+                           cudaStream_t st) {
+    k_count_fallback<<<1, 1, 0, st>>>(iters, first, configured, fallback, total);
 }
 
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st) {

@@ -28,7 +28,8 @@ void launch_features(const KParams& p, const float4* x, const float4* v, const i
                      cudaStream_t st);
 void launch_gather_rows(const int* slots, int count, int n, const float* feat, const float* lam_acc, float* out_feat,
                         float* out_target, int* err, cudaStream_t st);
-void launch_count_fallback(const int* iters, int first, int configured, int* fallback, cudaStream_t st);
+void launch_count_fallback(const int* iters, int first, int configured, int* fallback, long long* total,
+                           cudaStream_t st);
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st);
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
                  cudaStream_t st);

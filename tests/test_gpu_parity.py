@@ -223,11 +223,14 @@ def test_adaptive_iterations_reach_tolerance():
     sc = scenes.dam_break(16, (40, 20, 20), stable=True, iterations=1)
     s = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(adaptive=1, density_tol=0.005, max_iterations=12))
     s.upload(sc.pos, sc.vel)
-    for _ in range(4):
+    total = 0
+    for k in range(4):
         s.step(1)
         st = s.stats()
         assert st["max_density_error"] <= 0.005 or st["last_iterations"] == 12
         assert 1 <= st["last_iterations"] <= 12
+        total += st["last_iterations"]
+        assert st["substeps"] == k + 1 and st["total_iterations"] == total
     pos, _ = s.download()
     mx, _ = O.density_error(pos, float(sc.para.h), float(sc.para.restRho))
     assert mx <= 0.005 + 1e-4 or st["last_iterations"] == 12

@@ -163,3 +163,17 @@ def test_oracle_pair_lane_sums_depart_only_by_rounding(lanes):
     scale = a.get("rho").max() / float(sc.para.restRho) / float(sc.para.epsilon)
     assert np.abs(lam_a - lam_b).max() <= 1e-5 * scale
     assert np.abs(a.get("x") - b.get("x")).max() <= 1e-5 * np.abs(a.get("x")).max()
+
+
+def test_soft_rsqrt_within_two_ulp():
+    """The product arithmetic's reciprocal square root (bit-level estimate plus
+    three Newton steps) against double precision, over the |r|^2 range of the
+    neighbour sums and a wide sweep of binades."""
+    rng = np.random.RandomState(5)
+    xs = np.concatenate([rng.uniform(1e-6, 1.0, 4000), 2.0 ** rng.uniform(-60, 60, 4000)]).astype(np.float32)
+    worst = 0.0
+    for x in xs:
+        y = np.float32(O.rsqrt(float(x)))
+        exact = 1.0 / math.sqrt(float(x))
+        worst = max(worst, abs(float(y) - exact) / float(np.spacing(np.float32(exact))))
+    assert worst <= 2.0, worst
