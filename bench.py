@@ -35,6 +35,11 @@ UNIT = "particle-substeps/s"
 L2_FLUSH_BYTES = 256 << 20
 # algorithmic bytes per particle and launch (12-byte vectors, each array read or written once)
 ALG_BYTES = {"hash": 16, "reorder": 80, "lambda": 16, "dp": 28, "curl": 36, "vort": 48, "neighbors": 12}
+# algorithmic bytes of the HBM-bound kernels of this design, per particle (scan: per cell key):
+# hash reads x, v and writes cell, ticket; scatter reads cell, ticket, the cell start and writes
+# one slot; reorder reads x, v, cell, perm, the cell start, the cell's slot and writes x, v,
+# x_old, perm and the sorted cell; scan reads a count and writes a start and a cleared count
+MEM_BYTES = {"hash": 32, "scatter": 16, "reorder": 84, "scan_per_key": 12}
 # algorithmic flops per neighbour pair (FMA = 2)
 ALG_FLOPS_PER_PAIR = {"lambda": 30, "dp": 40, "curl": 25, "vort": 30}
 
@@ -299,6 +304,7 @@ def run_b200(args) -> int:
     e2e_value = n * world * args.steps / e2e_s
 
     hbm_peak, peak_kind, mp = peaks()
+    nkeys_main = solver.ncells + 1
     dom = max(("lambda", "dp", "neighbors", "curl", "vort"), key=lambda s: stages.get(s, 0.0))
     per_launch = {"lambda": 4, "dp": 4}.get(dom, 1)
     launch_ms = stages[dom] / per_launch
@@ -327,6 +333,7 @@ def run_b200(args) -> int:
                           "frac_hbm": step_bytes / (tot_s / args.steps) / 1e9 / hbm_peak},
         "stages_ms": {k: round(v, 5) for k, v in stages.items()},
         "stages_note": "per-kernel CUDA-event times from a profiled pass over the same K substeps and state",
+        "membound": membound_table(stages, n, nkeys_main, hbm_peak),
         "autotune": dict(autotune.ext_for(tuned), table=tuned["table"]),
         "value_l2_warm": n * world * args.steps / warm_s,
         "density_error": {"max": statistics.mean(e[0] for e in errs), "worst": max(e[0] for e in errs),
@@ -508,9 +515,38 @@ def measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, wei
         out[label] = {"min_iterations": iters, "particles": total, "value": total * args.steps / t, "unit": UNIT,
                       "ms_per_step": 1e3 * t / args.steps, "density_error": err,
                       "mean_iterations": (st["total_iterations"] - before["total_iterations"]) / args.steps}
+        if label == "plain":
+            # per-kernel times of the same substeps on a profiled handle
+            pos_s, vel_s = b.download()
+            prof = BatchSolver(para, descs, scenes.default_ext(profile=1, **ov))
+            prof.upload(pos_s, vel_s)
+            acc = {}
+            for _ in range(args.steps):
+                flush.zero_()
+                prof.step(1, stream)
+                for name, ms in prof.stage_times().items():
+                    acc[name] = acc.get(name, 0.0) + ms
+            nkeys = sum(prof.scene_layout(i)["ncells"] + 1 for i in range(prof.nscenes))
+            prof.close()
+            stages = {k: v / args.steps for k, v in acc.items() if v > 0}
+            out[label]["stages_ms"] = {k: round(v, 5) for k, v in stages.items()}
+            out[label]["membound"] = membound_table(stages, sum(x.n for x in mine), nkeys, peaks()[0])
         if kw.get("adaptive"):
             out[label]["density_tol"] = kw["density_tol"]
         b.close()
+    return out
+
+
+def membound_table(stages: dict, n: int, nkeys: int, peak: float) -> dict:
+    """Achieved bandwidth of the HBM-bound kernels from per-launch stage times (ms)."""
+    out = {}
+    for name in ("hash", "scan", "scatter", "reorder"):
+        ms = stages.get(name)
+        if not ms:
+            continue
+        b = MEM_BYTES["scan_per_key"] * nkeys if name == "scan" else MEM_BYTES[name] * n
+        gbs = b / (ms * 1e-3) / 1e9
+        out[name] = {"ms": round(ms, 5), "alg_bytes": b, "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
     return out
 
 

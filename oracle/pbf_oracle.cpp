@@ -151,6 +151,10 @@ template <typename T> inline T dot_fma(const V3<T>& a, const V3<T>& b) {
 template <typename T> inline V3<T> cross(const V3<T>& a, const V3<T>& b) {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
+// product (the curl's pair term): one fused multiply-add per component
+template <typename T> inline V3<T> cross_fma(const V3<T>& a, const V3<T>& b) {
+    return {std::fma(a.y, b.z, -(a.z * b.y)), std::fma(a.z, b.x, -(a.x * b.z)), std::fma(a.x, b.y, -(a.y * b.x))};
+}
 
 template <typename T> struct Consts {
     T h, h2, invH, poly6_c, spiky_c, wdq, inv_wdq, nk, rho0, rho0sq, eps, dt, jit, rmin, visc_c, vort_eps;
@@ -276,12 +280,13 @@ public:
             return {s * r.x, s * r.y, s * r.z};
         }
         if (p.arith == 1) {
-            // product: y = rsqrt(|r|^2) by soft_rsqrt, |r| = |r|^2 y, s = c (h-|r|)^2 y
+            // product: y = rsqrt(|r|^2) by soft_rsqrt, |r| = |r|^2 y for the cutoff,
+            // h - |r| = fma(-|r|^2, y, h), s = c (h-|r|)^2 y
             const float r2 = (float)dot_fma(r, r);
             const float y = soft_rsqrt(std::max(r2, 1e-30f));
             const float rl = r2 * y;
             if (rl > (float)k.h || rl < (float)k.rmin) return {0, 0, 0};
-            const float d = (float)k.h - rl;
+            const float d = std::fma(-r2, y, (float)k.h);
             const float s = (((float)k.spiky_c * d) * d) * y;
             return {(T)(s * (float)r.x), (T)(s * (float)r.y), (T)(s * (float)r.z)};
         }
@@ -312,6 +317,19 @@ public:
         }
         if (p.formulation == 0) return (T)(-p.k * powf((float)w / (float)k.wdq, p.n) * p.scorr_scale);
         return (T)(-p.k * std::pow((float)w / (float)k.wdq, p.n) * p.scorr_scale);
+    }
+
+    // product: the dp pair weight (lambda_i + lambda_j) + Scorr as one fused multiply-add
+    T dp_weight(T li, T lj, T w) const {
+        const T q = w * k.inv_wdq;
+        T pw;
+        if (k.n_int > 0) {
+            pw = q;
+            for (int i = 1; i < k.n_int; ++i) pw = pw * q;
+        } else {
+            pw = (T)powf((float)q, p.n);
+        }
+        return std::fma(k.nk * pw, (T)p.scorr_scale, li + lj);
     }
 
     // randomOffset: kernels/cudaPBFSolver.cuh:112-119 (GPU), include/solver.h:62-69 (CPU)
@@ -606,7 +624,9 @@ public:
                     const V3<T> d = sub(x[i], x[j]);
                     const T w = W6(d);
                     const V3<T> g = gradW(d);
-                    const T s = (lambda[i] + lambda[j]) + scorr(w);
+                    // product: fma(-k (W/W(dq))^n, scorr_scale, lambda_i + lambda_j)
+                    const T s = (p.arith == 1 && !is_double) ? dp_weight(lambda[i], lambda[j], w)
+                                                             : (lambda[i] + lambda[j]) + scorr(w);
                     if (p.arith == 1 && !is_double) {
                         a.x = std::fma(s, g.x, a.x);
                         a.y = std::fma(s, g.y, a.y);
@@ -659,7 +679,8 @@ public:
                     const int j = nb(i)[q];
                     // GPU: (v_j - v_i) x gradW ; CPU: (v_i - v_j) x gradW
                     const V3<T> vij = p.formulation == 0 ? sub(v[j], v[i]) : sub(v[i], v[j]);
-                    const V3<T> c = cross(vij, gradW(sub(x[i], x[j])));
+                    const V3<T> g = gradW(sub(x[i], x[j]));
+                    const V3<T> c = pa ? cross_fma(vij, g) : cross(vij, g);
                     w = {w.x + c.x, w.y + c.y, w.z + c.z};
                 }
                 wl[t] = w;

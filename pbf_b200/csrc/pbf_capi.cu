@@ -134,6 +134,7 @@ KParams make_kparams(const pbf_solver& s) {
     k.h = p.h;
     k.h2 = p.h * p.h;
     const float cs = p.h * e.cell_scale;
+    k.cell = cs;
     k.inv_cell = 1.0f / cs;
     k.poly6_c = (float)(315.0 * inv_pi_ref / (64.0 * std::pow((double)p.h, 9)));
     k.spiky_c = (float)(-45.0 * inv_pi_ref / std::pow((double)p.h, 6));
@@ -311,8 +312,7 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
     int first = 0;
     if (feats && iters > 0) {
         P(ST_LAMBDA, [&] {
-            launch_features(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->cell_start, s->lam_prev_sorted, s->Q, s->feat,
-                            s->lam_acc, st);
+            launch_features(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->lam_prev_sorted, s->Q, s->feat, s->lam_acc, st);
         });
         if (warm)
             P(ST_MLP, [&] {
@@ -364,10 +364,9 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
     }
     P(ST_CURL, [&] { launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, st); });
     P(ST_VORT, [&] {
-        launch_vort(kp, dbg, s->Px, s->Pv, s->omega, s->nbr, s->ncnt, s->Sv, s->Pperm, s->Sperm, s->vort_dbg,
-                    s->visc_dbg, st);
+        launch_vort(kp, dbg, s->Px, s->Pv, s->omega, s->nbr, s->ncnt, s->Sx, s->Sv, s->Pperm, s->Sperm,
+                    s->vort_dbg, s->visc_dbg, st);
     });
-    P(ST_COPY, [&] { launch_copy4(n, s->Px, s->Sx, st); });
 }
 
 int build_graph(pbf_solver* s) {

@@ -10,8 +10,13 @@
 // Formulas follow the reference CUDA kernels (kernels/cudaPBFSolver.cuh:99-181,
 // kernels/cudaPBFSolver.cu:4-239); the departures in evaluation order are:
 //   * poly6: (h^2-r^2)^3 by two multiplies instead of powf(.,3) (cuh:102)
-//   * spiky gradient: one reciprocal square root y = pbf_rsqrt(|r|^2), |r| = |r|^2 y,
-//     s = c (h-|r|)^2 y, then s * r, instead of powf(.,2) and normalize (cuh:106-109)
+//   * spiky gradient: one reciprocal square root y = pbf_rsqrt(|r|^2), |r| = |r|^2 y
+//     for the cutoff, h - |r| = fma(-|r|^2, y, h), s = c (h-|r|)^2 y, then s * r,
+//     instead of powf(.,2) and normalize (cuh:106-109)
+//   * the dp pair weight (lambda_i + lambda_j) + s_corr as one fused multiply-add,
+//     fma(-k (W/W(dq))^n, scorr_scale, lambda_i + lambda_j) (cu:193-195)
+//   * the curl's cross product with one fused multiply-add per component,
+//     fma(a_y, b_z, -(a_z b_y)) and its rotations (cu:211)
 //   * s_corr exponent: repeated multiplication for integer n in [1,8] (cuh:143)
 //   * |r|^2 and every neighbour sum use fused multiply-adds in a fixed order
 //   * the wall-jitter hash evaluates sine with pbf_det_sin (double precision)
@@ -54,7 +59,7 @@ struct SceneView {
 
 struct KParams {
     // kernel constants, all computed on the host (pbf_capi.cu: make_kparams)
-    float h, h2, inv_cell, poly6_c, spiky_c, inv_wdq, nk, scorr_scale, n_exp;
+    float h, h2, cell, inv_cell, poly6_c, spiky_c, inv_wdq, nk, scorr_scale, n_exp;
     float rho0, rho0sq, eps, dt, jit, rmin, visc_c, vort_eps;
     float g[3];
     SceneView sc0;              // the scene when there is one
@@ -158,29 +163,17 @@ __device__ __forceinline__ float pbf_rsqrt(float x) {
     return y;
 }
 
-// WspikyGrad (cuh:105-110): zero when |r| > h or |r| < rmin, else ((c*d)*d)/|r| * r.
-// |r|^2 is clamped to 1e-30 first so that coincident particles give |r| ~ 0
-// (cut by rmin) instead of an infinite estimate.
+// WspikyGrad (cuh:105-110): zero when |r| > h or |r| < rmin, else ((c*d)*d)/|r| * r
+// with d = h - |r|. |r|^2 is clamped to 1e-30 first so that coincident particles
+// give |r| ~ 0 (cut by rmin) instead of an infinite estimate. (The pair passes in
+// pbf_pairs.cu evaluate the same steps, two pairs per instruction.)
 __device__ __forceinline__ f3 grad_spiky(const KParams& p, const f3& r, float r2) {
     const float y = pbf_rsqrt(fmaxf(r2, 1e-30f));
     const float rl = r2 * y;
     if (rl > p.h || rl < p.rmin) return {0.0f, 0.0f, 0.0f};
-    const float d = p.h - rl;
+    const float d = __fmaf_rn(-r2, y, p.h);
     const float s = ((p.spiky_c * d) * d) * y;
     return {s * r.x, s * r.y, s * r.z};
-}
-
-// Scorr (cuh:142-144): -k (W / W(dq))^n, times scorr_scale
-__device__ __forceinline__ float s_corr(const KParams& p, float w) {
-    const float q = w * p.inv_wdq;
-    float pw;
-    if (p.n_int > 0) {
-        pw = q;
-        for (int i = 1; i < p.n_int; ++i) pw = pw * q;
-    } else {
-        pw = powf(q, p.n_exp);
-    }
-    return (p.nk * pw) * p.scorr_scale;
 }
 
 // randomOffset (cuh:112-119) with pbf_det_sin in place of sinf

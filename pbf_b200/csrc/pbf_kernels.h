@@ -1,4 +1,6 @@
-// Host-side launchers of the substep kernels (pbf_kernels.cu).
+// Host-side launchers of the substep kernels (pbf_kernels.cu; the neighbour-sum
+// passes launch_lambda, launch_dp, launch_features, launch_curl and launch_vort
+// are in pbf_pairs.cu).
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -24,8 +26,7 @@ void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr
 void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, const int* ncnt, const float4* xold,
                float4* xout, float4* vout, float4* dp, const IterCtl& ctl, cudaStream_t st);
 void launch_features(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
-                     const int* cell_start, const float* lam_prev, float4* xl, float* feat, float* lam_acc,
-                     cudaStream_t st);
+                     const float* lam_prev, float4* xl, float* feat, float* lam_acc, cudaStream_t st);
 void launch_gather_rows(const int* slots, int count, int n, const float* feat, const float* lam_acc, float* out_feat,
                         float* out_target, int* err, cudaStream_t st);
 void launch_count_fallback(const int* iters, int first, int configured, int* fallback, long long* total,
@@ -33,9 +34,10 @@ void launch_count_fallback(const int* iters, int first, int configured, int* fal
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st);
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
                  cudaStream_t st);
+// Vorticity + XSPH; also writes the final state: xout = x, vout = v + dv, perm_out = perm_in.
 void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v, const float4* omega, const int* nbr,
-                 const int* ncnt, float4* vout, const int* perm_in, int* perm_out, float4* vort, float4* visc,
-                 cudaStream_t st);
+                 const int* ncnt, float4* xout, float4* vout, const int* perm_in, int* perm_out, float4* vort,
+                 float4* visc, cudaStream_t st);
 void launch_density_error(const KParams& p, const float4* x, const int* nbr, const int* ncnt,
                           unsigned long long* max_bits, double* sum, const int* skip, cudaStream_t st);
 void launch_from_aos(int n, const float* pos, const float* vel, float4* x, float4* v, int* perm, int* err,

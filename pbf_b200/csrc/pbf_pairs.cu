@@ -1,0 +1,672 @@
+// Neighbour-sum passes of the PBF substep for sm_100a: density and lambda (with
+// the warm-start features in the first pass of a substep), the position
+// correction, curl, and vorticity confinement + XSPH.
+//
+// Reference kernels replaced (kernels/cudaPBFSolver.cu): calculateLambda
+// :156-180, calculateOffset :182-199, updatePosition :15-22, calculateCurl
+// :201-215, calculateVorticityAndViscosity :217-239, applyVorticityAndViscosity
+// :24-29.
+//
+// Pair lanes. A particle's neighbour list is split over P = L * V lanes: L
+// consecutive threads of a warp (a team), each evaluating V = 1 or 2 pairs per
+// instruction. With V = 2 the pair arithmetic runs on the sm_100 packed FP32
+// operations (add/mul/fma.rn.f32x2), each component of which is the scalar
+// IEEE operation, so one instruction evaluates two pairs and the
+// per-pair results are the scalar ones bit for bit. Lane p = V t + v (thread t,
+// component v) takes list entries p, p + P, p + 2P, ... in list order; the lane
+// sums are combined by an xor butterfly over distances 1, 2, 4 (first the two
+// components of a thread, then across the team by shuffles), which gives
+// ((s0 + s1) + (s2 + s3)) + ... on every lane. pair_lanes = P selects
+// (L, V): 1 = (1, 1), 2 = (1, 2), 4 = (2, 2), 8 = (4, 2).
+//
+// A padding component (an entry past the end of the list) contributes +0 to
+// every sum, which leaves the sum unchanged: no accumulator is ever -0 (they
+// start at +0, and in round-to-nearest x + (-x) = +0 and +0 + (-0) = +0).
+#include "pbf_kernels.h"
+
+#include <type_traits>
+
+namespace pbf {
+
+// ---- packed arithmetic: T = float (one pair) or float2 (two pairs) -------------
+// The float2 forms are the PTX f32x2 instructions with an explicit .rn rounding
+// modifier, which the compiler never contracts (a multiply feeding an add stays
+// two rounded operations, as in the scalar code built with -fmad=false).
+__device__ __forceinline__ unsigned long long as_u64(float2 a) {
+    return (unsigned long long)__float_as_uint(a.x) | ((unsigned long long)__float_as_uint(a.y) << 32);
+}
+__device__ __forceinline__ float2 as_f2(unsigned long long u) {
+    return make_float2(__uint_as_float((unsigned)u), __uint_as_float((unsigned)(u >> 32)));
+}
+__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
+    return as_f2(d);
+}
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
+    return as_f2(d);
+}
+__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)), "l"(as_u64(c)));
+    return as_f2(d);
+}
+__device__ __forceinline__ float vneg(float a) { return -a; }
+__device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
+// a - b is a + (-b) exactly, signed zeros included
+template <typename T> __device__ __forceinline__ T vsub(T a, T b) { return vadd(a, vneg(b)); }
+__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ float2 vmax(float2 a, float b) { return make_float2(fmaxf(a.x, b), fmaxf(a.y, b)); }
+
+template <typename T> __device__ __forceinline__ T bc(float s);
+template <> __device__ __forceinline__ float bc<float>(float s) { return s; }
+template <> __device__ __forceinline__ float2 bc<float2>(float s) { return make_float2(s, s); }
+
+// bit v set: component v greater than / less than s
+__device__ __forceinline__ unsigned gt_mask(float a, float s) { return a > s ? 1u : 0u; }
+__device__ __forceinline__ unsigned gt_mask(float2 a, float s) { return (a.x > s ? 1u : 0u) | (a.y > s ? 2u : 0u); }
+__device__ __forceinline__ unsigned lt_mask(float a, float s) { return a < s ? 1u : 0u; }
+__device__ __forceinline__ unsigned lt_mask(float2 a, float s) { return (a.x < s ? 1u : 0u) | (a.y < s ? 2u : 0u); }
+// components whose bit in keep is clear become +0
+__device__ __forceinline__ float keep_only(float a, unsigned keep) { return (keep & 1u) ? a : 0.0f; }
+__device__ __forceinline__ float2 keep_only(float2 a, unsigned keep) {
+    return make_float2((keep & 1u) ? a.x : 0.0f, (keep & 2u) ? a.y : 0.0f);
+}
+// the first butterfly step: the two lanes of a thread
+__device__ __forceinline__ float fold(float a) { return a; }
+__device__ __forceinline__ float fold(float2 a) { return a.x + a.y; }
+
+// pbf_rsqrt (pbf_device.cuh) on each component
+__device__ __forceinline__ float vrsqrt(float x) { return pbf_rsqrt(x); }
+__device__ __forceinline__ float2 vrsqrt(float2 x) {
+    const float2 hx = vmul(bc<float2>(0.5f), x);
+    float2 y = make_float2(__int_as_float(0x5f3759df - (__float_as_int(x.x) >> 1)),
+                           __int_as_float(0x5f3759df - (__float_as_int(x.y) >> 1)));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) y = vmul(y, vfma(vneg(hx), vmul(y, y), bc<float2>(1.5f)));
+    return y;
+}
+
+template <typename T> struct T3 {
+    T x, y, z;
+};
+template <typename T> __device__ __forceinline__ T3<T> add3(const T3<T>& a, const T3<T>& b) {
+    return {vadd(a.x, b.x), vadd(a.y, b.y), vadd(a.z, b.z)};
+}
+template <typename T> __device__ __forceinline__ T3<T> zero3() { return {bc<T>(0.0f), bc<T>(0.0f), bc<T>(0.0f)}; }
+__device__ __forceinline__ f3 fold3(const T3<float>& a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ f3 fold3(const T3<float2>& a) { return {fold(a.x), fold(a.y), fold(a.z)}; }
+// The curl's cross product, one fused multiply-add per component:
+// (fma(a_y, b_z, -(a_z b_y)), fma(a_z, b_x, -(a_x b_z)), fma(a_x, b_y, -(a_y b_x))).
+// (A packed multiply whose only use is an add may be fused by the code generator,
+// so every product that meets an addition in these passes is an explicit fma.)
+template <typename T> __device__ __forceinline__ T3<T> cross3v(const T3<T>& a, const T3<T>& b) {
+    return {vfma(a.y, b.z, vneg(vmul(a.z, b.y))), vfma(a.z, b.x, vneg(vmul(a.x, b.z))),
+            vfma(a.x, b.y, vneg(vmul(a.y, b.x)))};
+}
+
+// xyz (or .w) of V gathered float4s as one packet
+__device__ __forceinline__ T3<float> pack3(const float4 (&a)[1]) { return {a[0].x, a[0].y, a[0].z}; }
+__device__ __forceinline__ T3<float2> pack3(const float4 (&a)[2]) {
+    return {make_float2(a[0].x, a[1].x), make_float2(a[0].y, a[1].y), make_float2(a[0].z, a[1].z)};
+}
+__device__ __forceinline__ float packw(const float4 (&a)[1]) { return a[0].w; }
+__device__ __forceinline__ float2 packw(const float4 (&a)[2]) { return make_float2(a[0].w, a[1].w); }
+
+template <int V> using vec_t = typename std::conditional<V == 1, float, float2>::type;
+
+// r = x_k - x_j, |r|^2 = fma(z, z, fma(y, y, x*x)), Wpoly6 (when NEED_W) and the
+// spiky gradient of V pairs, exactly as w_poly6 / grad_spiky (pbf_device.cuh)
+// evaluate one pair; components outside `valid` give w = +0 and g = +0.
+template <typename T, bool NEED_W>
+__device__ __forceinline__ void pair_terms(const KParams& p, const f3& xk, const T3<T>& xj, unsigned valid, T3<T>& r,
+                                           T& w, T3<T>& g) {
+    r = {vsub(bc<T>(xk.x), xj.x), vsub(bc<T>(xk.y), xj.y), vsub(bc<T>(xk.z), xj.z)};
+    const T r2 = vfma(r.z, r.z, vfma(r.y, r.y, vmul(r.x, r.x)));
+    if (NEED_W) {
+        const T t = vsub(bc<T>(p.h2), r2);
+        w = keep_only(vmul(bc<T>(p.poly6_c), vmul(vmul(t, t), t)), valid & ~gt_mask(r2, p.h2));
+    }
+    const T y = vrsqrt(vmax(r2, 1e-30f));
+    const T rl = vmul(r2, y);                  // |r| for the cutoff
+    const T d = vfma(vneg(r2), y, bc<T>(p.h));  // h - |r|
+    const T s = vmul(vmul(vmul(bc<T>(p.spiky_c), d), d), y);
+    const unsigned keep = valid & ~(gt_mask(rl, p.h) | lt_mask(rl, p.rmin));
+    g = {keep_only(vmul(s, r.x), keep), keep_only(vmul(s, r.y), keep), keep_only(vmul(s, r.z), keep)};
+}
+
+// The dp pair weight (lambda_i + lambda_j) + s_corr (cu:193-195, Scorr cuh:142-144)
+// as fma(-k (W / W(dq))^n, scorr_scale, lambda_i + lambda_j).
+__device__ __forceinline__ float vpow(float q, const KParams& p) { return powf(q, p.n_exp); }
+__device__ __forceinline__ float2 vpow(float2 q, const KParams& p) {
+    return make_float2(powf(q.x, p.n_exp), powf(q.y, p.n_exp));
+}
+template <typename T> __device__ __forceinline__ T dp_weight(const KParams& p, float li, T lj, T w) {
+    const T q = vmul(w, bc<T>(p.inv_wdq));
+    T pw;
+    if (p.n_int > 0) {
+        pw = q;
+        for (int i = 1; i < p.n_int; ++i) pw = vmul(pw, q);
+    } else {
+        pw = vpow(q, p);
+    }
+    return vfma(vmul(bc<T>(p.nk), pw), bc<T>(p.scorr_scale), vadd(bc<T>(li), lj));
+}
+
+// ---- teams -------------------------------------------------------------------
+template <int L> struct Team {
+    int k;          // particle slot
+    int t;          // thread within the team
+    unsigned mask;  // the team's lanes within the warp
+};
+
+// blockDim.x is a multiple of 32, so a team never straddles a warp
+template <int L> __device__ __forceinline__ Team<L> team_of() {
+    Team<L> m;
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    m.k = (int)(g / L);
+    m.t = (int)(threadIdx.x & (L - 1));
+    const int lane = threadIdx.x & 31;
+    m.mask = L >= 32 ? 0xffffffffu : (((1u << L) - 1u) << (lane & ~(L - 1)));
+    return m;
+}
+
+// the butterfly across the team (distances 1, 2 between threads)
+template <int L> __device__ __forceinline__ float team_sum(float v, unsigned mask) {
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+template <int L> __device__ __forceinline__ f3 team_sum3(f3 v, unsigned mask) {
+    return {team_sum<L>(v.x, mask), team_sum<L>(v.y, mask), team_sum<L>(v.z, mask)};
+}
+
+// Entries q0 + u P + v (u < B, v < V) of slot k's list; slot k itself past the
+// end (its data is then masked). All index loads of a batch are issued before
+// the gathers that depend on them.
+template <int V, int P, int B>
+__device__ __forceinline__ void load_idx(const KParams& p, const int* __restrict__ nbr, int k, int q0, int cnt,
+                                         int (&jj)[B][V]) {
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int q = q0 + u * P + v;
+            jj[u][v] = q < cnt ? nbr[(size_t)q * p.stride + k] : k;
+        }
+}
+
+// bit v: entry q + v exists
+template <int V> __device__ __forceinline__ unsigned valid_bits(int q, int cnt) {
+    return V == 1 ? 1u : ((q < cnt ? 1u : 0u) | (q + 1 < cnt ? 2u : 0u));
+}
+
+// Block-wide max and sum of a per-thread error, folded into one slot with a
+// single pair of atomics per block (max as ordered double bits, value >= 0).
+__device__ __forceinline__ void block_error_reduce(float e, unsigned long long* max_bits, double* sum) {
+    __shared__ float s_max[32];
+    __shared__ float s_sum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float m = e, s = e;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    if (lane == 0) { s_max[warp] = m; s_sum[warp] = s; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double dsum = 0.0;
+        for (int w = 0; w < nw; ++w) { m = fmaxf(m, s_max[w]); dsum += (double)s_sum[w]; }
+        atomicMax(max_bits, (unsigned long long)__double_as_longlong((double)m));
+        atomicAdd(sum, dsum);
+    }
+}
+
+// Neighbour entries in flight per thread and batch: four (two in the vorticity
+// pass, which gathers three float4s per entry).
+template <int V> __host__ __device__ constexpr int batches() { return 4 / V; }
+
+// ---------------------------------------------------------------------------
+// a9: density, constraint and lambda (calculateLambda cu:156-180), with the
+// one-sided density error of the positions it sees
+// ---------------------------------------------------------------------------
+template <bool DEBUG, int L, int V>
+__global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_lambda(KParams p, const float4* __restrict__ x, const int* __restrict__ nbr,
+                                                const int* __restrict__ ncnt, float4* __restrict__ xl,
+                                                float* __restrict__ rho_out, IterCtl ctl) {
+    using T = vec_t<V>;
+    constexpr int P = L * V, B = batches<V>();
+    if (ctl.done && *ctl.done) return;
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    float err = 0.0f;
+    if (k < p.n) {
+        const f3 xk = make3(x[k]);
+        const int cnt = ncnt[k];
+        T rho = bc<T>(0.0f), gm = bc<T>(0.0f);
+        T3<T> gs = zero3<T>();
+        for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
+            int jj[B][V];
+            load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
+            float4 xj[B][V];
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+#pragma unroll
+                for (int v = 0; v < V; ++v) xj[u][v] = x[jj[u][v]];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int q = q0 + u * P;
+                if (q >= cnt) break;
+                T3<T> r, g;
+                T w;
+                pair_terms<T, true>(p, xk, pack3(xj[u]), valid_bits<V>(q, cnt), r, w, g);
+                rho = vadd(rho, w);
+                gs = add3(gs, g);
+                gm = vfma(g.x, g.x, gm);
+                gm = vfma(g.y, g.y, gm);
+                gm = vfma(g.z, g.z, gm);
+            }
+        }
+        float rhos = team_sum<L>(fold(rho), tm.mask);
+        float gms = team_sum<L>(fold(gm), tm.mask);
+        f3 g3 = team_sum3<L>(fold3(gs), tm.mask);
+        if (tm.t == 0) {
+            // one-sided error of the fluid density at these positions (no wall term)
+            err = fmaxf(__fdiv_rn(rhos, p.rho0) - 1.0f, 0.0f);
+            if (p.flags & FLAG_WALL_DENSITY) {
+                f3 gw;
+                rhos = rhos + wall_term(p, scene_of(p, k), xk, gw);
+                g3 = {g3.x + gw.x, g3.y + gw.y, g3.z + gw.z};
+            }
+            float C = __fdiv_rn(rhos, p.rho0) - 1.0f;
+            if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
+            gms = __fmaf_rn(g3.x, g3.x, gms);
+            gms = __fmaf_rn(g3.y, g3.y, gms);
+            gms = __fmaf_rn(g3.z, g3.z, gms);
+            gms = __fdiv_rn(gms, p.rho0sq);
+            const float lam = __fdiv_rn(-C, gms + p.eps);
+            xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
+            if (ctl.lam_acc) ctl.lam_acc[k] += lam;
+            if (DEBUG) rho_out[k] = rhos;
+        }
+    }
+    if (ctl.max_bits) block_error_reduce(err, ctl.max_bits, ctl.sum);
+}
+
+// ---------------------------------------------------------------------------
+// a17: warm-start features (no reference counterpart), computed in the first
+// lambda pass of a substep together with that pass's lambda (the same
+// arithmetic as k_lambda, so recording features changes no result):
+//   0 neighbour count / cap          1 fluid density / rho0
+//   2 previous substep's total lambda
+//   3 sum |grad C|^2 (the lambda denominator without eps)
+//   4 velocity divergence sum (v_j - v_i) . grad W / rho0 (predicted velocities)
+//   5-7 distance to the nearer wall per axis / h, clamped to [0, 4]
+//   8 neighbours closer than h/2, / cap
+//   9 |sum of (x_i - x_j)| / (h max(count, 1))  (offset of the neighbourhood)
+//   10 |sum grad W| h / rho0
+//   11 sum |v_j - v_i|^2 (dt / h)^2 / max(count, 1)
+// None depends on the grid's cell size. lam_acc starts the substep's total lambda
+// at this pass's lambda.
+// ---------------------------------------------------------------------------
+template <int L, int V>
+__global__ void __launch_bounds__(256) k_features(KParams p, const float4* __restrict__ x,
+                                                  const float4* __restrict__ v, const int* __restrict__ nbr,
+                                                  const int* __restrict__ ncnt, const float* __restrict__ lam_prev,
+                                                  float4* __restrict__ xl, float* __restrict__ feat,
+                                                  float* __restrict__ lam_acc) {
+    using T = vec_t<V>;
+    constexpr int P = L * V, B = batches<V>();
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
+    const f3 xk = make3(x[k]);
+    const f3 vk = make3(v[k]);
+    const int cnt = ncnt[k];
+    T rho = bc<T>(0.0f), gm = bc<T>(0.0f), div = bc<T>(0.0f), close = bc<T>(0.0f), dv2 = bc<T>(0.0f);
+    T3<T> gs = zero3<T>(), rs = zero3<T>();
+    const float q2 = 0.25f * p.h2;
+    for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
+        int jj[B][V];
+        load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
+        float4 xj[B][V], vj[B][V];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+#pragma unroll
+            for (int c = 0; c < V; ++c) {
+                xj[u][c] = x[jj[u][c]];
+                vj[u][c] = v[jj[u][c]];
+            }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int q = q0 + u * P;
+            if (q >= cnt) break;
+            const unsigned valid = valid_bits<V>(q, cnt);
+            T3<T> r, g;
+            T w;
+            pair_terms<T, true>(p, xk, pack3(xj[u]), valid, r, w, g);
+            rho = vadd(rho, w);
+            gs = add3(gs, g);
+            gm = vfma(g.x, g.x, gm);
+            gm = vfma(g.y, g.y, gm);
+            gm = vfma(g.z, g.z, gm);
+            const T3<T> vv = pack3(vj[u]);
+            const T3<T> vji = {vsub(vv.x, bc<T>(vk.x)), vsub(vv.y, bc<T>(vk.y)), vsub(vv.z, bc<T>(vk.z))};
+            div = vfma(vji.x, g.x, div);
+            div = vfma(vji.y, g.y, div);
+            div = vfma(vji.z, g.z, div);
+            const T r2 = vfma(r.z, r.z, vfma(r.y, r.y, vmul(r.x, r.x)));
+            close = vadd(close, keep_only(bc<T>(1.0f), valid & lt_mask(r2, q2)));
+            rs = add3(rs, T3<T>{keep_only(r.x, valid), keep_only(r.y, valid), keep_only(r.z, valid)});
+            dv2 = vadd(dv2, keep_only(vfma(vji.z, vji.z, vfma(vji.y, vji.y, vmul(vji.x, vji.x))), valid));
+        }
+    }
+    float rhos = team_sum<L>(fold(rho), tm.mask);
+    float gms = team_sum<L>(fold(gm), tm.mask);
+    f3 g3 = team_sum3<L>(fold3(gs), tm.mask);
+    const float divs = team_sum<L>(fold(div), tm.mask);
+    const float closes = team_sum<L>(fold(close), tm.mask);
+    const f3 r3 = team_sum3<L>(fold3(rs), tm.mask);
+    const float dv2s = team_sum<L>(fold(dv2), tm.mask);
+    if (tm.t != 0) return;
+    const SceneView sc = scene_of(p, k);
+    const float rho_fluid = rhos;
+    const float gsl = __fsqrt_rn(dot_fma(g3, g3));
+    if (p.flags & FLAG_WALL_DENSITY) {
+        f3 gw;
+        rhos = rhos + wall_term(p, sc, xk, gw);
+        g3 = {g3.x + gw.x, g3.y + gw.y, g3.z + gw.z};
+    }
+    float C = __fdiv_rn(rhos, p.rho0) - 1.0f;
+    if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
+    gms = __fmaf_rn(g3.x, g3.x, gms);
+    gms = __fmaf_rn(g3.y, g3.y, gms);
+    gms = __fmaf_rn(g3.z, g3.z, gms);
+    gms = __fdiv_rn(gms, p.rho0sq);
+    const float lam = __fdiv_rn(-C, gms + p.eps);
+    xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
+    lam_acc[k] = lam;
+
+    const float inv_cnt = 1.0f / (float)max(cnt, 1);
+    float f[12];
+    f[0] = (float)cnt / (float)p.max_nbr;
+    f[1] = rho_fluid / p.rho0;
+    f[2] = lam_prev[k];
+    f[3] = gms;
+    f[4] = divs / p.rho0;
+    const float qa[3] = {xk.x, xk.y, xk.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float dw = fminf(qa[a] - sc.bmin[a], sc.bmax[a] - qa[a]) * p.inv_h;
+        f[5 + a] = fminf(fmaxf(dw, 0.0f), 4.0f);
+    }
+    f[8] = closes / (float)p.max_nbr;
+    f[9] = __fsqrt_rn(dot_fma(r3, r3)) * p.inv_h * inv_cnt;
+    f[10] = gsl * p.h / p.rho0;
+    const float dth = p.dt * p.inv_h;
+    f[11] = dv2s * (dth * dth) * inv_cnt;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) feat[(size_t)k * 12 + i] = f[i];
+}
+
+// ---------------------------------------------------------------------------
+// a10 + a11: position correction with tensile s_corr, then x += dp, wall clamp,
+// and on the last iteration v = (x - x_old) / dt
+// (calculateOffset cu:182-199, updatePosition cu:15-22)
+// ---------------------------------------------------------------------------
+template <bool DEBUG, int L, int V>
+__global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_dp(KParams p, const float4* __restrict__ xl, const int* __restrict__ nbr,
+                                            const int* __restrict__ ncnt, const float4* __restrict__ xold,
+                                            float4* __restrict__ xout, float4* __restrict__ vout,
+                                            float4* __restrict__ dp_out, IterCtl ctl) {
+    using T = vec_t<V>;
+    constexpr int P = L * V, B = batches<V>();
+    if (ctl.done) {
+        if (*ctl.done) return;
+        // the lambda pass just measured the positions this pass would correct;
+        // when they are within tolerance the loop ends here
+        if (ctl.may_stop && __longlong_as_double((long long)*ctl.max_bits) <= ctl.tol) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                *ctl.done = 1;
+                *ctl.conv_slot = ctl.slot;
+            }
+            return;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ctl.iters, 1);
+    }
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
+    const float4 xk4 = xl[k];
+    const f3 xk = make3(xk4);
+    const float lk = xk4.w;
+    const int cnt = ncnt[k];
+    T3<T> a = zero3<T>();
+    for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
+        int jj[B][V];
+        load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
+        float4 xj[B][V];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+#pragma unroll
+            for (int c = 0; c < V; ++c) xj[u][c] = xl[jj[u][c]];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int q = q0 + u * P;
+            if (q >= cnt) break;
+            T3<T> r, g;
+            T w;
+            pair_terms<T, true>(p, xk, pack3(xj[u]), valid_bits<V>(q, cnt), r, w, g);
+            const T s = dp_weight(p, lk, packw(xj[u]), w);
+            a = {vfma(s, g.x, a.x), vfma(s, g.y, a.y), vfma(s, g.z, a.z)};
+        }
+    }
+    f3 as = team_sum3<L>(fold3(a), tm.mask);
+    if (tm.t != 0) return;
+    if (p.flags & FLAG_WALL_DENSITY) {
+        f3 gw;
+        wall_term(p, scene_of(p, k), xk, gw);
+        as.x = __fmaf_rn(lk, gw.x, as.x);
+        as.y = __fmaf_rn(lk, gw.y, as.y);
+        as.z = __fmaf_rn(lk, gw.z, as.z);
+    }
+    const f3 dp = {__fdiv_rn(as.x, p.rho0), __fdiv_rn(as.y, p.rho0), __fdiv_rn(as.z, p.rho0)};
+    f3 xn = {xk.x + dp.x, xk.y + dp.y, xk.z + dp.z};
+    bound_particle(p, scene_of(p, k), xn);
+    xout[k] = make_float4(xn.x, xn.y, xn.z, 0.0f);
+    if (vout) {
+        const float4 xo = xold[k];
+        vout[k] = make_float4(__fdiv_rn(xn.x - xo.x, p.dt), __fdiv_rn(xn.y - xo.y, p.dt),
+                              __fdiv_rn(xn.z - xo.z, p.dt), 0.0f);
+    }
+    if (DEBUG) dp_out[k] = make_float4(dp.x, dp.y, dp.z, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// a12: vorticity (calculateCurl cu:201-215): w_i = sum (v_j - v_i) x gradW(x_i - x_j);
+// |w_i| goes to .w for the vorticity pass
+// ---------------------------------------------------------------------------
+template <int L, int V>
+__global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
+                                              const int* __restrict__ nbr, const int* __restrict__ ncnt,
+                                              float4* __restrict__ omega) {
+    using T = vec_t<V>;
+    constexpr int P = L * V, B = batches<V>();
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
+    const f3 xk = make3(x[k]);
+    const f3 vk = make3(v[k]);
+    const int cnt = ncnt[k];
+    T3<T> wsum = zero3<T>();
+    for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
+        int jj[B][V];
+        load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
+        float4 xj[B][V], vj[B][V];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+#pragma unroll
+            for (int c = 0; c < V; ++c) {
+                xj[u][c] = x[jj[u][c]];
+                vj[u][c] = v[jj[u][c]];
+            }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int q = q0 + u * P;
+            if (q >= cnt) break;
+            T3<T> r, g;
+            T w;
+            pair_terms<T, false>(p, xk, pack3(xj[u]), valid_bits<V>(q, cnt), r, w, g);
+            const T3<T> vv = pack3(vj[u]);
+            const T3<T> vji = {vsub(vv.x, bc<T>(vk.x)), vsub(vv.y, bc<T>(vk.y)), vsub(vv.z, bc<T>(vk.z))};
+            wsum = add3(wsum, cross3v(vji, g));
+        }
+    }
+    const f3 w3 = team_sum3<L>(fold3(wsum), tm.mask);
+    if (tm.t == 0) omega[k] = make_float4(w3.x, w3.y, w3.z, __fsqrt_rn(dot_fma(w3, w3)));
+}
+
+// ---------------------------------------------------------------------------
+// a13: vorticity confinement and XSPH, applied to v
+// (calculateVorticityAndViscosity cu:217-239, applyVorticityAndViscosity cu:24-29);
+// also writes the substep's final state (x, v, perm) for the next substep
+// ---------------------------------------------------------------------------
+template <bool DEBUG, int L, int V>
+__global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
+                                              const float4* __restrict__ omega, const int* __restrict__ nbr,
+                                              const int* __restrict__ ncnt, float4* __restrict__ xout,
+                                              float4* __restrict__ vout, const int* __restrict__ perm_in,
+                                              int* __restrict__ perm_out, float4* __restrict__ vort_out,
+                                              float4* __restrict__ visc_out) {
+    using T = vec_t<V>;
+    constexpr int P = L * V, B = 2 / V;  // three 16-byte gathers per entry
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    if (k >= p.n) return;  // uniform over the team
+    const f3 xk = make3(x[k]);
+    const f3 vk = make3(v[k]);
+    const int cnt = ncnt[k];
+    T3<T> pv = zero3<T>(), eta = zero3<T>();
+    for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
+        int jj[B][V];
+        load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
+        float4 xj[B][V], vj[B][V], oj[B][V];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+#pragma unroll
+            for (int c = 0; c < V; ++c) {
+                xj[u][c] = x[jj[u][c]];
+                vj[u][c] = v[jj[u][c]];
+                oj[u][c] = omega[jj[u][c]];
+            }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int q = q0 + u * P;
+            if (q >= cnt) break;
+            T3<T> r, g;
+            T w;
+            pair_terms<T, true>(p, xk, pack3(xj[u]), valid_bits<V>(q, cnt), r, w, g);
+            const T3<T> vv = pack3(vj[u]);
+            const T3<T> vji = {vsub(vv.x, bc<T>(vk.x)), vsub(vv.y, bc<T>(vk.y)), vsub(vv.z, bc<T>(vk.z))};
+            pv = {vfma(vji.x, w, pv.x), vfma(vji.y, w, pv.y), vfma(vji.z, w, pv.z)};
+            const T wl = packw(oj[u]);  // |w_j| (k_curl)
+            eta = {vfma(wl, g.x, eta.x), vfma(wl, g.y, eta.y), vfma(wl, g.z, eta.z)};
+        }
+    }
+    const f3 pvs = team_sum3<L>(fold3(pv), tm.mask);
+    f3 etas = team_sum3<L>(fold3(eta), tm.mask);
+    if (tm.t != 0) return;
+    const float el = __fsqrt_rn(dot_fma(etas, etas));
+    if ((double)el > 1e-3) etas = {__fdiv_rn(etas.x, el), __fdiv_rn(etas.y, el), __fdiv_rn(etas.z, el)};
+    const f3 cr = cross3(etas, make3(omega[k]));
+    const f3 fv = {p.vort_eps * cr.x, p.vort_eps * cr.y, p.vort_eps * cr.z};
+    const f3 vs = {p.visc_c * pvs.x, p.visc_c * pvs.y, p.visc_c * pvs.z};
+    const f3 t = {p.dt * fv.x + vs.x, p.dt * fv.y + vs.y, p.dt * fv.z + vs.z};
+    xout[k] = make_float4(xk.x, xk.y, xk.z, 0.0f);
+    vout[k] = make_float4(vk.x + t.x, vk.y + t.y, vk.z + t.z, 0.0f);
+    perm_out[k] = perm_in[k];
+    if (DEBUG) {
+        vort_out[k] = make_float4(fv.x, fv.y, fv.z, 0.0f);
+        visc_out[k] = make_float4(vs.x, vs.y, vs.z, 0.0f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+// blocks for n particles with L threads each
+static inline int team_blocks(int n, int L, int bs) { return (int)(((long long)n * L + bs - 1) / bs); }
+
+// Calls f with (L, V) of pair_lanes as compile-time constants.
+template <int A, int B> struct LV {
+    static constexpr int L = A, V = B;
+};
+template <typename F> void with_lanes(int lanes, F&& f) {
+    switch (lanes) {
+        case 1: f(LV<1, 1>{}); break;
+        case 4: f(LV<2, 2>{}); break;
+        case 8: f(LV<4, 2>{}); break;
+        default: f(LV<1, 2>{}); break;
+    }
+}
+
+void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr, const int* ncnt, float4* xl,
+                   float* rho, const IterCtl& ctl, cudaStream_t st) {
+    with_lanes(p.lanes, [&](auto c) {
+        constexpr int L = decltype(c)::L, V = decltype(c)::V;
+        const int b = team_blocks(p.n, L, p.block);
+        if (debug) k_lambda<true, L, V><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+        else k_lambda<false, L, V><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+    });
+}
+
+void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, const int* ncnt, const float4* xold,
+               float4* xout, float4* vout, float4* dp, const IterCtl& ctl, cudaStream_t st) {
+    with_lanes(p.lanes, [&](auto c) {
+        constexpr int L = decltype(c)::L, V = decltype(c)::V;
+        const int b = team_blocks(p.n, L, p.block);
+        if (debug) k_dp<true, L, V><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+        else k_dp<false, L, V><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+    });
+}
+
+void launch_features(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
+                     const float* lam_prev, float4* xl, float* feat, float* lam_acc, cudaStream_t st) {
+    with_lanes(p.lanes, [&](auto c) {
+        constexpr int L = decltype(c)::L, V = decltype(c)::V;
+        k_features<L, V><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, lam_prev, xl, feat,
+                                                                            lam_acc);
+    });
+}
+
+void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
+                 cudaStream_t st) {
+    with_lanes(p.lanes, [&](auto c) {
+        constexpr int L = decltype(c)::L, V = decltype(c)::V;
+        k_curl<L, V><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, omega);
+    });
+}
+
+void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v, const float4* omega, const int* nbr,
+                 const int* ncnt, float4* xout, float4* vout, const int* perm_in, int* perm_out, float4* vort,
+                 float4* visc, cudaStream_t st) {
+    with_lanes(p.lanes, [&](auto c) {
+        constexpr int L = decltype(c)::L, V = decltype(c)::V;
+        const int b = team_blocks(p.n, L, p.block);
+        if (debug)
+            k_vort<true, L, V><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort,
+                                                      visc);
+        else
+            k_vort<false, L, V><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, xout, vout, perm_in, perm_out,
+                                                       vort, visc);
+    });
+}
+
+}  // namespace pbf

@@ -23,7 +23,7 @@ NUM_B = _lib.MLP_NUM_BIASES
 W1, W2, W3, W4 = 0, 64 * 16, 64 * 16 + 64 * 64, 64 * 16 + 2 * 64 * 64
 B1, B2, B3, B4, FMEAN, FISTD, OSCALE = 0, 64, 128, 192, 193, 209, 225
 FEATURES = ["neighbour_fraction", "density", "previous_total_lambda", "grad_c_sq", "divergence", "wall_x",
-            "wall_y", "wall_z", "own_cell", "mean_cell", "nonempty_cells", "max_cell"]
+            "wall_y", "wall_z", "close_fraction", "neighbourhood_offset", "grad_w_sum", "velocity_spread"]
 
 
 def init_params(seed: int = 0):

@@ -98,7 +98,6 @@ def test_features_match_cpu_recomputation():
     xp = s.fetch("xpred")[:, :3].astype(np.float64)
     ncnt = s.fetch("ncnt")
     nbr = s.fetch("nbr").reshape(s.max_neighbors, s.stride)
-    cs = s.fetch("cell_start")
     h, rho0 = float(sc.para.h), float(sc.para.restRho)
     assert np.allclose(f[:, 0], ncnt / 63.0, rtol=0, atol=1e-7)
     # previous substep's total lambda, carried through the re-sort
@@ -116,28 +115,33 @@ def test_features_match_cpu_recomputation():
         r2 = ((xp[m] - xp[j]) ** 2).sum(1)
         rho[m] += np.where(r2 <= h * h, c6 * np.maximum(h * h - r2, 0) ** 3, 0.0)
     assert np.allclose(f[:, 1], rho / rho0, rtol=2e-5, atol=1e-6)
-    # wall distances and the 27-cell occupancy statistics
+    # wall distances
     lo, hi = np.array(sc.boundary[:3]), np.array(sc.boundary[3:])
     dw = np.clip(np.minimum(xp - lo, hi - xp) / h, 0, 4)
     assert np.allclose(f[:, 5:8], dw, atol=1e-5)
-    dims = np.array(sc.ext_overrides["grid_dims"])
-    d = np.floor(xp / h).astype(int)
-    occ = cs[1:] - cs[:-1]
-    for k in range(0, s.n, 97):
-        vals = []
-        own = 0
-        for dz in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dx in (-1, 0, 1):
-                    c = d[k] + (dx, dy, dz)
-                    if np.any(c < 0) or np.any(c >= dims):
-                        continue
-                    o = occ[c[0] + c[1] * dims[0] + c[2] * dims[0] * dims[1]]
-                    vals.append(o)
-                    if dx == dy == dz == 0:
-                        own = o
-        assert f[k, 8] == own and abs(f[k, 9] - sum(vals) / 27.0) < 1e-5
-        assert abs(f[k, 10] - sum(v > 0 for v in vals) / 27.0) < 1e-6 and f[k, 11] == max(vals)
+    # close neighbours, neighbourhood offset and |sum grad W| from the same lists
+    close = np.zeros(s.n)
+    roff = np.zeros((s.n, 3))
+    gsum = np.zeros((s.n, 3))
+    spiky = -45.0 / (np.pi * h ** 6)
+    for q in range(s.max_neighbors):
+        m = ncnt > q
+        if not m.any():
+            break
+        j = nbr[q, : s.n][m]
+        r = xp[m] - xp[j]
+        r2 = (r ** 2).sum(1)
+        close[m] += r2 < 0.25 * h * h
+        roff[m] += r
+        rl = np.sqrt(r2)
+        ok = (rl <= h) & (rl >= 0.01)
+        coef = np.where(ok, spiky * (h - rl) ** 2 / np.maximum(rl, 1e-30), 0.0)
+        gsum[m] += coef[:, None] * r
+    assert np.array_equal(f[:, 8], (close / 63.0).astype(np.float32))
+    cnt1 = np.maximum(ncnt, 1)
+    assert np.allclose(f[:, 9], np.linalg.norm(roff, axis=1) / (h * cnt1), rtol=1e-4, atol=1e-5)
+    assert np.allclose(f[:, 10], np.linalg.norm(gsum, axis=1) * h / rho0, rtol=1e-3, atol=1e-4)
+    assert np.all(np.isfinite(f[:, 11])) and np.all(f[:, 11] >= 0)
 
 
 def _run_errors(sc, ext, steps, w16=None, b32=None):
