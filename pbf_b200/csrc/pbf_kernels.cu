@@ -38,12 +38,18 @@ __global__ void __launch_bounds__(256) k_hash(KParams p, const float4* __restric
         if (!(isfinite(xi.x) && isfinite(xi.y) && isfinite(xi.z))) atomicOr(err, DEVERR_NONFINITE);
         key = cell_key(p, sc, xi);
     }
-    // warp-aggregated histogram: one atomic per distinct cell in the warp
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
-    const int leader = __ffs(peers) - 1;
-    const int rank = __popc(peers & ((1u << lane) - 1u));
+    // Run-aggregated histogram: slots are in cell order from the previous substep,
+    // so equal keys come in runs; one atomic per run of equal keys in the warp.
+    // (The ticket is only an arrival order; k_reorder makes the order stable.)
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+    const unsigned upto = starts & (0xffffffffu >> (31 - lane));  // run starts at or below this lane
+    const int leader = 31 - __clz(upto);
+    const unsigned above = starts & ~(0xffffffffu >> (31 - lane));
+    const int end = above ? __ffs(above) - 1 : 32;  // first run start above this lane
+    const int rank = lane - leader;
     int base = 0;
-    if (key >= 0 && lane == leader) base = atomicAdd(&cnt[key], __popc(peers));
+    if (key >= 0 && lane == leader) base = atomicAdd(&cnt[key], end - leader);
     base = __shfl_sync(0xffffffffu, base, leader);
     if (i < p.n) {
         cell[i] = key;
@@ -73,6 +79,9 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
     return v;
 }
 
+// VEC: cnt and out are 16-byte aligned; each lane moves four consecutive counts
+// per access (int4), four rounds of 128 per warp instead of sixteen of 32.
+template <bool VEC>
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, int* __restrict__ out, int m,
                                                        unsigned long long* __restrict__ status,
                                                        int* __restrict__ tile_counter, int* __restrict__ err,
@@ -85,28 +94,59 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
     __syncthreads();
     const int tile = s_tile;
 
-    // Warp w owns elements [tile * TILE + w * 512, +512) in 16 rounds of 32
-    // consecutive elements (one coalesced 128-byte access per round); each round
-    // is scanned across the warp and carried into the next.
+    // Warp w owns elements [tile * TILE + w * 512, +512) in rounds of consecutive
+    // elements (coalesced: 32 counts per round, or 128 as int4 when VEC); each
+    // round is scanned across the warp and carried into the next.
     const long long wbase = (long long)tile * SCAN_TILE + (long long)warp * (32 * SCAN_ITEMS);
     int item[SCAN_ITEMS];
+    int carry = 0;  // warp-exclusive offset of the round
+    if (VEC) {
 #pragma unroll
-    for (int q = 0; q < SCAN_ITEMS; ++q) {
-        const long long idx = wbase + q * 32 + lane;
-        item[q] = idx < m ? cnt[idx] : 0;
-    }
-    int carry = 0;  // warp-exclusive offset of round q
+        for (int r = 0; r < SCAN_ITEMS / 4; ++r) {
+            const long long i0 = wbase + r * 128 + lane * 4;
+            if (i0 + 3 < m) {
+                const int4 q = *reinterpret_cast<const int4*>(cnt + i0);
+                item[4 * r] = q.x; item[4 * r + 1] = q.y; item[4 * r + 2] = q.z; item[4 * r + 3] = q.w;
+            } else {
 #pragma unroll
-    for (int q = 0; q < SCAN_ITEMS; ++q) {
-        int incl = item[q];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+                for (int e = 0; e < 4; ++e) item[4 * r + e] = i0 + e < m ? cnt[i0 + e] : 0;
+            }
         }
-        const int excl_q = carry + incl - item[q];
-        carry += __shfl_sync(0xffffffffu, incl, 31);
-        item[q] = excl_q;  // now the exclusive prefix within the warp's range
+#pragma unroll
+        for (int r = 0; r < SCAN_ITEMS / 4; ++r) {
+            const int a0 = item[4 * r], a1 = a0 + item[4 * r + 1], a2 = a1 + item[4 * r + 2];
+            const int tot = a2 + item[4 * r + 3];
+            int incl = tot;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int ex = carry + incl - tot;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+            item[4 * r] = ex;  // exclusive prefixes within the warp's range
+            item[4 * r + 1] = ex + a0;
+            item[4 * r + 2] = ex + a1;
+            item[4 * r + 3] = ex + a2;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < SCAN_ITEMS; ++q) {
+            const long long idx = wbase + q * 32 + lane;
+            item[q] = idx < m ? cnt[idx] : 0;
+        }
+#pragma unroll
+        for (int q = 0; q < SCAN_ITEMS; ++q) {
+            int incl = item[q];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int excl_q = carry + incl - item[q];
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+            item[q] = excl_q;  // now the exclusive prefix within the warp's range
+        }
     }
     if (lane == 0) s_warp[warp] = carry;  // the warp's total
     __syncthreads();
@@ -166,12 +206,31 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
     }
     __syncthreads();
     const int off = s_excl + s_warp[warp];
+    if (VEC) {
 #pragma unroll
-    for (int q = 0; q < SCAN_ITEMS; ++q) {
-        const long long idx = wbase + q * 32 + lane;
-        if (idx < m) {
-            out[idx] = off + item[q];
-            if (clear) cnt[idx] = 0;
+        for (int r = 0; r < SCAN_ITEMS / 4; ++r) {
+            const long long i0 = wbase + r * 128 + lane * 4;
+            if (i0 + 3 < m) {
+                *reinterpret_cast<int4*>(out + i0) =
+                    make_int4(off + item[4 * r], off + item[4 * r + 1], off + item[4 * r + 2], off + item[4 * r + 3]);
+                if (clear) *reinterpret_cast<int4*>(cnt + i0) = make_int4(0, 0, 0, 0);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (i0 + e < m) {
+                        out[i0 + e] = off + item[4 * r + e];
+                        if (clear) cnt[i0 + e] = 0;
+                    }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < SCAN_ITEMS; ++q) {
+            const long long idx = wbase + q * 32 + lane;
+            if (idx < m) {
+                out[idx] = off + item[q];
+                if (clear) cnt[idx] = 0;
+            }
         }
     }
     if (tile == (int)(((long long)m - 1) / SCAN_TILE) && threadIdx.x == SCAN_THREADS - 1) {
@@ -456,6 +515,7 @@ __global__ void k_copy4(int n, const float4* __restrict__ a, float4* __restrict_
 // launchers
 // ---------------------------------------------------------------------------
 static inline int blocks_for(int n, int bs) { return (n + bs - 1) / bs; }
+static inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 void launch_hash(const KParams& p, bool predict_on, const float4* x, const float4* v, int* cell, int* ticket, int* cnt,
                  int* err, cudaStream_t st) {
     const int b = blocks_for(p.n, 256);
@@ -473,7 +533,8 @@ void launch_scan(int* cnt, int* out, int m, void* status_ws, int* err, cudaStrea
     unsigned long long* status = (unsigned long long*)status_ws;
     int* counter = (int*)(status + tiles);
     cudaMemsetAsync(status_ws, 0, scan_status_bytes(m), st);
-    k_scan<<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, 1);
+    if (aligned16(cnt) && aligned16(out)) k_scan<true><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, 1);
+    else k_scan<false><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, 1);
 }
 
 void launch_scan_const(const int* in, int* out, int m, void* status_ws, int* err, cudaStream_t st) {
@@ -481,7 +542,10 @@ void launch_scan_const(const int* in, int* out, int m, void* status_ws, int* err
     unsigned long long* status = (unsigned long long*)status_ws;
     int* counter = (int*)(status + tiles);
     cudaMemsetAsync(status_ws, 0, scan_status_bytes(m), st);
-    k_scan<<<tiles, SCAN_THREADS, 0, st>>>(const_cast<int*>(in), out, m, status, counter, err, 0);
+    if (aligned16(in) && aligned16(out))
+        k_scan<true><<<tiles, SCAN_THREADS, 0, st>>>(const_cast<int*>(in), out, m, status, counter, err, 0);
+    else
+        k_scan<false><<<tiles, SCAN_THREADS, 0, st>>>(const_cast<int*>(in), out, m, status, counter, err, 0);
 }
 
 void launch_scatter(int n, const int* cell, const int* ticket, const int* cell_start, int* tmp, int* err,

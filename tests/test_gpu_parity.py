@@ -207,6 +207,28 @@ def test_scan_matches_exclusive_prefix(m):
     assert np.array_equal(d_in.cpu().numpy(), a), "input must be left unchanged"
 
 
+@pytest.mark.parametrize("m", [1, 4099, 262144 + 3])
+@pytest.mark.parametrize("shift", [1, 3])
+def test_scan_unaligned_pointers(m, shift):
+    """Arrays that do not start on a 16-byte boundary take the scalar path of the
+    scan (aligned ones move four counts per access); both give the same prefix."""
+    import torch
+    from pbf_b200._lib import lib, check
+    rng = np.random.RandomState(m + shift)
+    a = rng.randint(0, 16, size=m).astype(np.int32)
+    buf_in = torch.zeros(m + 8, dtype=torch.int32, device="cuda")
+    buf_in[shift:shift + m] = torch.from_numpy(a).cuda()
+    buf_out = torch.full((m + 8,), -7, dtype=torch.int32, device="cuda")
+    ws_bytes = lib().pbf_scan_workspace_bytes(m)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    check(lib().pbf_scan_exclusive_i32(buf_in[shift:].data_ptr(), buf_out[shift:].data_ptr(), m, ws.data_ptr(),
+                                       ws_bytes, None))
+    want = np.concatenate([[0], np.cumsum(a, dtype=np.int64)]).astype(np.int32)
+    out = buf_out.cpu().numpy()
+    assert np.array_equal(out[shift:shift + m + 1], want)
+    assert np.all(out[:shift] == -7) and np.all(out[shift + m + 1:] == -7)
+
+
 def test_density_error_vs_fp64_oracle():
     sc = scenes.dam_break(16, (40, 20, 20), stable=True, iterations=4)
     s = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(measure_error=1))
