@@ -178,7 +178,13 @@ def run_reference(args) -> int:
     return 0
 
 
-def workload_config(args) -> dict:
+def workload_config(args, sc=None) -> dict:
+    if args.main_scene == "large":
+        return {"workload": f"double dam break {sc.n}: two 128^3 lattices, sphere r=20h, box 320h x 160h x 160h, "
+                            "rho0 6378, eps 600, 4 Jacobi iterations, dt 1/120, stable mode",
+                "particles": sc.n, "iterations": 4, "grid": [320, 160, 160],
+                "l2": "inputs larger than L2, and flushed before every timed step (256 MiB write)",
+                "parallelism": f"{args.gpus} independent replicas" if args.gpus > 1 else "single scene"}
     return {"workload": "dam_break_262144: 64^3 lattice, spacing 0.5h, jitter 0.01h, h=0.1, box 80h x 40h x 40h, "
                         "rho0 6378, eps 600, 4 Jacobi iterations, dt 1/120, stable mode",
             "particles": 262144, "iterations": 4, "grid": [80, 40, 40],
@@ -214,7 +220,10 @@ def run_b200(args) -> int:
         return float(t.item())
 
     from pbf_b200 import autotune
-    sc = scenes.config1(seed=rank, iterations=4)
+    if args.main_scene == "large":
+        sc = scenes.config4(seed=rank, iterations=4, n_small=0)[0]
+    else:
+        sc = scenes.config1(seed=rank, iterations=4)
     n = sc.n
     stream = torch.cuda.current_stream()
     if args.pair_lanes and args.cell_scale and args.block_size:
@@ -319,7 +328,7 @@ def run_b200(args) -> int:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * tot_s / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jittered lattice)",
-        "config": workload_config(args),
+        "config": workload_config(args, sc),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 12 * n,
                 "note": "pinned host positions+velocities in, upload, one substep, positions out, every step"},
         "gpu_launches": kernels * args.steps,
@@ -572,6 +581,9 @@ def main() -> int:
     ap.add_argument("--pair-lanes", type=int, default=0, help="with --cell-scale and --block-size: skip the "
                     "autotuner of the single-scene leg and use these launch settings")
     ap.add_argument("--cell-scale", type=float, default=0.0)
+    ap.add_argument("--main-scene", choices=["config1", "large"], default="config1",
+                    help="scene of the single-scene leg: the 262,144-particle dam break (the headline) or the "
+                         "4,194,304-particle double dam break with the sphere (for profiling at scale)")
     ap.add_argument("--block-size", type=int, default=0)
     args = ap.parse_args()
     if args.impl == "reference":

@@ -22,7 +22,7 @@ namespace pbf {
 // a1 + a2: predict, bound, hash, histogram (one arrival ticket per particle)
 // ---------------------------------------------------------------------------
 template <bool PREDICT>
-__global__ void __launch_bounds__(256) k_hash(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
+__global__ void __launch_bounds__(256, 8) k_hash(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
                                               int* __restrict__ cell, int* __restrict__ ticket, int* __restrict__ cnt,
                                               int* __restrict__ err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256) k_hash(KParams p, const float4* __restric
 // bounded anyway and reports DEVERR_SCAN_TIMEOUT.
 // ---------------------------------------------------------------------------
 constexpr int SCAN_THREADS = 256;
-constexpr int SCAN_ITEMS = 16;
+constexpr int SCAN_ITEMS = 32;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr long long SCAN_SPIN_LIMIT = 1ll << 22;
 
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(256) k_scatter(int n, const int* __restrict__ 
 }
 
 template <bool PREDICT>
-__global__ void __launch_bounds__(256) k_reorder(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
+__global__ void __launch_bounds__(256, 8) k_reorder(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
                                                  const int* __restrict__ perm, const int* __restrict__ cell,
                                                  const int* __restrict__ cell_start, const int* __restrict__ tmp,
                                                  float4* __restrict__ xp, float4* __restrict__ vp,

@@ -5,7 +5,7 @@
 // application that owns every device allocation through its own pool, or code
 // running with a device-memory budget fixed at start-up. For them this entry
 // point runs the same decoupled look-back scan as pbf_scan_exclusive_i32 with
-// its scratch (one status word per 4,096-element tile, a tile counter and an
+// its scratch (one status word per tile of the scan, a tile counter and an
 // error word) in a file-scope device array instead of a caller workspace.
 //
 // The array is a static __device__ object: every GPU that loads this library
@@ -25,8 +25,8 @@
 
 namespace {
 
-constexpr int kMaxTiles = 4096;                       // tiles of 4,096 elements
-constexpr long long kMaxElements = 4096ll * kMaxTiles;  // 16,777,216
+constexpr int kMaxTiles = 4096;                         // room for 4,096 status words
+constexpr long long kMaxElements = 16777216ll;          // largest n accepted
 constexpr int kScratchBytes = kMaxTiles * 8 + 16 + 64;  // status words, counter, error word
 
 static __device__ __align__(256) unsigned char g_scan_scratch[kScratchBytes];
@@ -68,6 +68,8 @@ int pbf_scan_exclusive_i32_noalloc(const int* d_in, int* d_out, int n, void* str
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     const size_t status = pbf::scan_status_bytes(n);  // status words and tile counter
+    if (((status + 15) & ~(size_t)15) + sizeof(int) > (size_t)kScratchBytes)
+        return fail(PBF_ERR_INVALID, "n needs more scan tiles than the allocation-free scratch holds");
     int* err = (int*)((char*)scratch + ((status + 15) & ~(size_t)15));
     if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return fail(PBF_ERR_CUDA, "clearing the error word");
     pbf::launch_scan_const(d_in, d_out, n, scratch, err, st);  // clears the status words, then scans
