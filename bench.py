@@ -353,6 +353,8 @@ def run_b200(args) -> int:
         "clocks": clocks,
     }
     legs = set(args.legs.split(","))
+    if legs & {"all", "render"}:
+        out["render"] = measure_render(args, solver, sc, stream)
     if legs & {"all", "batched", "learned", "large"}:
         out["batched"] = measure_batched(args, rank, world, dev, flush, stream, barrier, max_over_ranks)
     if legs & {"all", "learned", "large"}:
@@ -559,6 +561,32 @@ def membound_table(stages: dict, n: int, nkeys: int, peak: float) -> dict:
     return out
 
 
+def measure_render(args, solver, sc, stream) -> dict:
+    """Headless screen-space rendering of the single-scene state (the reference
+    app's passes: sprite depth, 60 smoothing passes, thickness, normals, room,
+    shading) at 800 x 800, timed with CUDA events per frame."""
+    import torch
+
+    from pbf_b200 import render
+    w = h = 800
+    cam = render.box_camera(sc.grid_space, w, h, float(sc.para.radius), smooth_iterations=60)
+    r = render.Renderer(w, h)
+    for _ in range(3):
+        r.frame(cam, solver=solver, stream=stream)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for a, b in ev:
+        a.record(stream)
+        r.frame(cam, solver=solver, stream=stream)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
+    covered = int((r.read("depth_raw") > 0).sum())
+    r.close()
+    return {"width": w, "height": h, "smooth_iterations": 60, "particles": sc.n, "ms_per_frame": ms,
+            "frames_per_s": 1e3 / ms, "covered_pixels": covered}
+
+
 def load_traffic(kernel: str):
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
     path = os.path.join(REPO, "profiles", "traffic.json")
@@ -576,7 +604,7 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--legs", default="all",
-                    help="comma list of legs after the single-scene one: all, batched, learned, large, cpu "
+                    help="comma list of legs after the single-scene one: all, batched, learned, large, cpu, render "
                          "(main = the single-scene leg alone)")
     ap.add_argument("--pair-lanes", type=int, default=0, help="with --cell-scale and --block-size: skip the "
                     "autotuner of the single-scene leg and use these launch settings")

@@ -279,11 +279,55 @@ int pbf_tc_gemm_bf16(const void* d_a, const void* d_b, float* d_d, int n, int k,
  * the input is left unchanged. Synchronises `stream`. */
 int pbf_scan_exclusive_i32_noalloc(const int* d_in, int* d_out, int n, void* stream);
 
+/* ---- headless screen-space fluid rendering ----------------------------------
+ * The reference draws the fluid with OpenGL shader passes (src/renderapp.cpp:
+ * 400-466): point-sprite depth (shaders/depth.vert, depth.frag), 60 curvature-
+ * flow smoothing passes (smooth.frag), additive thickness (thickness.frag),
+ * normals from depth (normal.frag), the room (background.frag) and the fluid
+ * shading (shadingParticle.frag). Here each pass is a CUDA kernel writing device
+ * images of width x height pixels (row 0 at the bottom, as in the GL window). */
+typedef struct pbf_render pbf_render;
+
+typedef struct pbf_camera {
+    float view[16];            /* world -> view, column-major (glm::lookAt) */
+    float proj[16];            /* view -> clip, column-major (glm::perspective) */
+    float cam_pos[3];          /* eye position, world */
+    float radius;              /* sprite radius, world units (SolverParameter.radius) */
+    float point_coeff;         /* sprite size in pixels = -point_coeff * radius / z_view */
+    float tan_half_fov;        /* surface reconstruction of the shading pass */
+    float light_pos[3];        /* fluid light, world (reference (0, 50, -20)) */
+    float light_diffuse[3];    /* (0.8, 0.8, 0.8) */
+    float roi;                 /* Fresnel ratio (1.3) */
+    float room_light_pos[3];   /* room light, world (reference (0, 50, 0)) */
+    float room_light_diffuse[3];
+    float room[6];             /* room walls: xmin, ymin (floor), zmin (back), xmax, ymax, zmax */
+    int smooth_iterations;     /* curvature-flow passes (60) */
+    int reserved[5];
+} pbf_camera;
+
+/* images readable with pbf_render_read (floats per pixel in brackets) */
+#define PBF_IMAGE_DEPTH_RAW 0  /* [1] -z of the nearest sprite surface, 0 where empty */
+#define PBF_IMAGE_DEPTH 1      /* [1] after the smoothing passes */
+#define PBF_IMAGE_THICKNESS 2  /* [1] summed sprite thickness */
+#define PBF_IMAGE_NORMAL 3     /* [4] view-space normal xyz, 0 */
+#define PBF_IMAGE_ROOM 4       /* [4] room colour rgba (8-bit quantised, as the GL texture) */
+#define PBF_IMAGE_COLOR 5      /* [4] final colour rgba */
+
+int pbf_render_create(int width, int height, pbf_render** out);
+int pbf_render_destroy(pbf_render* r);
+/* Renders n particles whose xyz lie at d_pos + i * stride floats (stride 3 for
+ * AoS positions, 4 for float4) on `stream`. */
+int pbf_render_frame(pbf_render* r, const float* d_pos, int n, int stride, const pbf_camera* cam, void* stream);
+/* Renders a solver's current state. */
+int pbf_render_frame_solver(pbf_render* r, pbf_solver* s, const pbf_camera* cam, void* stream);
+/* Copies one image to host memory (count = floats available at host); synchronises. */
+int pbf_render_read(pbf_render* r, int image, float* host, size_t count);
+
 const char* pbf_last_error(void);
 int pbf_abi_version(void);
 
 /* sizeof of the ABI structs, for FFI bindings to check their layouts:
- * 0 pbf_solver_parameter, 1 pbf_ext_params, 2 pbf_stats. */
+ * 0 pbf_solver_parameter, 1 pbf_ext_params, 2 pbf_stats, 3 pbf_camera. */
 size_t pbf_struct_size(int which);
 
 #ifdef __cplusplus

@@ -71,6 +71,22 @@ class SceneDesc(C.Structure):
     ]
 
 
+class Camera(C.Structure):
+    """pbf_camera (include/pbf.h)."""
+
+    _fields_ = [
+        ("view", C.c_float * 16), ("proj", C.c_float * 16), ("cam_pos", C.c_float * 3), ("radius", C.c_float),
+        ("point_coeff", C.c_float), ("tan_half_fov", C.c_float), ("light_pos", C.c_float * 3),
+        ("light_diffuse", C.c_float * 3), ("roi", C.c_float), ("room_light_pos", C.c_float * 3),
+        ("room_light_diffuse", C.c_float * 3), ("room", C.c_float * 6), ("smooth_iterations", C.c_int),
+        ("reserved", C.c_int * 5),
+    ]
+
+
+IMAGE = {"depth_raw": 0, "depth": 1, "thickness": 2, "normal": 3, "room": 4, "color": 5}
+IMAGE_CHANNELS = {"depth_raw": 1, "depth": 1, "thickness": 1, "normal": 4, "room": 4, "color": 4}
+
+
 class Stats(C.Structure):
     _fields_ = [
         ("substeps", C.c_longlong), ("total_iterations", C.c_longlong), ("fallbacks", C.c_longlong),
@@ -120,6 +136,11 @@ _PROTOS = [
     ("pbf_scan_workspace_bytes", C.c_size_t, [C.c_int]),
     ("pbf_scan_exclusive_i32", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]),
     ("pbf_scan_exclusive_i32_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    ("pbf_render_create", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    ("pbf_render_destroy", C.c_int, [C.c_void_p]),
+    ("pbf_render_frame", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(Camera), C.c_void_p]),
+    ("pbf_render_frame_solver", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Camera), C.c_void_p]),
+    ("pbf_render_read", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
 ]
 
 

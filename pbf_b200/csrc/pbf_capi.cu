@@ -416,6 +416,7 @@ size_t pbf_struct_size(int which) {
         case 0: return sizeof(pbf_solver_parameter);
         case 1: return sizeof(pbf_ext_params);
         case 2: return sizeof(pbf_stats);
+        case 3: return sizeof(pbf_camera);
         default: return 0;
     }
 }
@@ -600,6 +601,17 @@ int create_common(const pbf_solver_parameter* para, int nscenes, const pbf_scene
 }
 
 }  // namespace
+
+namespace pbf {
+// Current positions of a solver (float4, slot order) for the renderer.
+int solver_positions(pbf_solver* s, const float4** x, int* n) {
+    if (!s) return set_last_error(PBF_ERR_INVALID, "null handle");
+    if (!s->uploaded) return set_last_error(PBF_ERR_STATE, "render before pbf_upload");
+    *x = s->Sx;
+    *n = s->n;
+    return PBF_OK;
+}
+}  // namespace pbf
 
 extern "C" {
 

@@ -7,6 +7,8 @@
 
 #include "pbf_device.cuh"
 
+struct pbf_solver;  // the solver handle of include/pbf.h
+
 namespace pbf {
 
 void launch_hash(const KParams& p, bool predict_on, const float4* x, const float4* v, int* cell, int* ticket, int* cnt,
@@ -47,5 +49,8 @@ void launch_copy4(int n, const float4* a, float4* b, cudaStream_t st);
 
 // Records the message returned by pbf_last_error() for this thread; returns code.
 int set_last_error(int code, const char* msg);
+
+// Current positions of a solver (float4, slot order) for the renderer (pbf_capi.cu).
+int solver_positions(::pbf_solver* s, const float4** x, int* n);
 
 }  // namespace pbf

@@ -31,6 +31,8 @@ def test_struct_layouts_match_the_c_side():
     assert L.pbf_struct_size(0) == C.sizeof(SolverParameter) == 52
     assert L.pbf_struct_size(1) == C.sizeof(ExtParams)
     assert L.pbf_struct_size(2) == C.sizeof(Stats)
+    from pbf_b200._lib import Camera
+    assert L.pbf_struct_size(3) == C.sizeof(Camera)
     assert L.pbf_abi_version() == 1
 
 
