@@ -89,7 +89,7 @@ struct pbf_solver {
     int* sid = nullptr;             // per slot: scene index (batches)
     // device state (slot order)
     float4 *Sx = nullptr, *Sv = nullptr, *Px = nullptr, *Pv = nullptr, *Pxold = nullptr, *Q = nullptr,
-           *omega = nullptr;
+           *omega = nullptr, *vw = nullptr;  // vw: v with |omega| in .w (curl -> vorticity)
     float4 *xpred_dbg = nullptr, *dp_dbg = nullptr, *vort_dbg = nullptr, *visc_dbg = nullptr;
     float* rho_dbg = nullptr;
     int *Sperm = nullptr, *Pperm = nullptr, *cell = nullptr, *ticket = nullptr, *tmp = nullptr,
@@ -193,7 +193,7 @@ template <typename T> int dalloc(T** p, size_t count) {
 }
 
 void free_all(pbf_solver* s) {
-    void* ptrs[] = {s->Sx, s->Sv, s->Px, s->Pv, s->Pxold, s->Q, s->omega, s->xpred_dbg, s->dp_dbg, s->vort_dbg,
+    void* ptrs[] = {s->Sx, s->Sv, s->Px, s->Pv, s->Pxold, s->Q, s->omega, s->vw, s->xpred_dbg, s->dp_dbg, s->vort_dbg,
                     s->visc_dbg, s->rho_dbg, s->Sperm, s->Pperm, s->cell, s->ticket, s->tmp, s->cell_sorted,
                     s->ncnt, s->nbr, s->cnt, s->cell_start, s->hash_dbg, s->lam_acc, s->lam_prev_sorted, s->lam0,
                     s->feat, s->scan_ws, s->dstats, s->staging, s->scenes_d, s->sid, s->mlp_w, s->mlp_b};
@@ -362,9 +362,9 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
         launch_count_fallback(&ds->iters, first, iters, &ds->fallback, &ds->total_iters, st);
         P(ST_VELOCITY, [&] { launch_velocity(kp, s->Px, s->Pxold, s->Pv, st); });
     }
-    P(ST_CURL, [&] { launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, st); });
+    P(ST_CURL, [&] { launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, s->vw, st); });
     P(ST_VORT, [&] {
-        launch_vort(kp, dbg, s->Px, s->Pv, s->omega, s->nbr, s->ncnt, s->Sx, s->Sv, s->Pperm, s->Sperm,
+        launch_vort(kp, dbg, s->Px, s->vw, s->omega, s->nbr, s->ncnt, s->Sx, s->Sv, s->Pperm, s->Sperm,
                     s->vort_dbg, s->visc_dbg, st);
     });
 }
@@ -550,7 +550,7 @@ int create_common(const pbf_solver_parameter* para, int nscenes, const pbf_scene
             return rc;                     \
         }                                  \
     } while (0)
-    AL(s->Sx, n); AL(s->Sv, n); AL(s->Px, n); AL(s->Pv, n); AL(s->Pxold, n); AL(s->Q, n); AL(s->omega, n);
+    AL(s->Sx, n); AL(s->Sv, n); AL(s->Px, n); AL(s->Pv, n); AL(s->Pxold, n); AL(s->Q, n); AL(s->omega, n); AL(s->vw, n);
     AL(s->Sperm, n); AL(s->Pperm, n); AL(s->cell, n); AL(s->ticket, n); AL(s->tmp, n); AL(s->cell_sorted, n);
     AL(s->ncnt, n);
     AL(s->nbr, (size_t)ext->max_neighbors * s->stride);

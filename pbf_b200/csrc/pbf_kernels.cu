@@ -15,6 +15,7 @@
 // setGrid :99-111, countingSort :112-122, buildNeighborhood :124-154; the
 // neighbour-sum passes (lambda, dp, curl, vorticity) are in pbf_pairs.cu.
 #include "pbf_kernels.h"
+#include "pbf_packed.cuh"
 
 namespace pbf {
 
@@ -345,19 +346,29 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
         s = cell_start[row + xa];
         e = cell_start[row + xb + 1];
     };
-    // candidates [s, e) in slot order, four positions in flight
+    // candidates [s, e) in slot order, four positions in flight; |r|^2 of two
+    // candidates per packed instruction (the same IEEE operations as dot_fma)
     auto scan_row = [&](int s, int e) {
         for (int j0 = s; j0 < e && c < cap; j0 += 4) {
             float4 xj[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) xj[u] = x[min(j0 + u, e - 1)];
+            float r2[4];
+#pragma unroll
+            for (int u = 0; u < 4; u += 2) {
+                const float2 rx = vsub(bc<float2>(xk.x), make_float2(xj[u].x, xj[u + 1].x));
+                const float2 ry = vsub(bc<float2>(xk.y), make_float2(xj[u].y, xj[u + 1].y));
+                const float2 rz = vsub(bc<float2>(xk.z), make_float2(xj[u].z, xj[u + 1].z));
+                const float2 d2 = vfma(rz, rz, vfma(ry, ry, vmul(rx, rx)));
+                r2[u] = d2.x;
+                r2[u + 1] = d2.y;
+            }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int j = j0 + u;
                 if (j >= e || c >= cap) break;
                 if (j == k) continue;
-                const f3 r = sub3(xk, make3(xj[u]));
-                if (dot_fma(r, r) <= p.h2) {
+                if (r2[u] <= p.h2) {
                     nbr[(size_t)c * p.stride + k] = j;
                     ++c;
                 }

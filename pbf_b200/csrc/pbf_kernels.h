@@ -34,10 +34,12 @@ void launch_gather_rows(const int* slots, int count, int n, const float* feat, c
 void launch_count_fallback(const int* iters, int first, int configured, int* fallback, long long* total,
                            cudaStream_t st);
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st);
+// Curl: omega = (w, |w|) and vw = (v, |w|) per particle.
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
-                 cudaStream_t st);
-// Vorticity + XSPH; also writes the final state: xout = x, vout = v + dv, perm_out = perm_in.
-void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v, const float4* omega, const int* nbr,
+                 float4* vw, cudaStream_t st);
+// Vorticity + XSPH from vw = (v, |w|) and omega; also writes the final state:
+// xout = x, vout = v + dv, perm_out = perm_in.
+void launch_vort(const KParams& p, bool debug, const float4* x, const float4* vw, const float4* omega, const int* nbr,
                  const int* ncnt, float4* xout, float4* vout, const int* perm_in, int* perm_out, float4* vort,
                  float4* visc, cudaStream_t st);
 void launch_density_error(const KParams& p, const float4* x, const int* nbr, const int* ncnt,

@@ -23,49 +23,11 @@
 // every sum, which leaves the sum unchanged: no accumulator is ever -0 (they
 // start at +0, and in round-to-nearest x + (-x) = +0 and +0 + (-0) = +0).
 #include "pbf_kernels.h"
+#include "pbf_packed.cuh"
 
 #include <type_traits>
 
 namespace pbf {
-
-// ---- packed arithmetic: T = float (one pair) or float2 (two pairs) -------------
-// The float2 forms are the PTX f32x2 instructions with an explicit .rn rounding
-// modifier, which the compiler never contracts (a multiply feeding an add stays
-// two rounded operations, as in the scalar code built with -fmad=false).
-__device__ __forceinline__ unsigned long long as_u64(float2 a) {
-    return (unsigned long long)__float_as_uint(a.x) | ((unsigned long long)__float_as_uint(a.y) << 32);
-}
-__device__ __forceinline__ float2 as_f2(unsigned long long u) {
-    return make_float2(__uint_as_float((unsigned)u), __uint_as_float((unsigned)(u >> 32)));
-}
-__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
-__device__ __forceinline__ float2 vadd(float2 a, float2 b) {
-    unsigned long long d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
-    return as_f2(d);
-}
-__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
-__device__ __forceinline__ float2 vmul(float2 a, float2 b) {
-    unsigned long long d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
-    return as_f2(d);
-}
-__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) {
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)), "l"(as_u64(c)));
-    return as_f2(d);
-}
-__device__ __forceinline__ float vneg(float a) { return -a; }
-__device__ __forceinline__ float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
-// a - b is a + (-b) exactly, signed zeros included
-template <typename T> __device__ __forceinline__ T vsub(T a, T b) { return vadd(a, vneg(b)); }
-__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
-__device__ __forceinline__ float2 vmax(float2 a, float b) { return make_float2(fmaxf(a.x, b), fmaxf(a.y, b)); }
-
-template <typename T> __device__ __forceinline__ T bc(float s);
-template <> __device__ __forceinline__ float bc<float>(float s) { return s; }
-template <> __device__ __forceinline__ float2 bc<float2>(float s) { return make_float2(s, s); }
 
 // bit v set: component v greater than / less than s
 __device__ __forceinline__ unsigned gt_mask(float a, float s) { return a > s ? 1u : 0u; }
@@ -491,12 +453,13 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_dp(KParams p, const flo
 
 // ---------------------------------------------------------------------------
 // a12: vorticity (calculateCurl cu:201-215): w_i = sum (v_j - v_i) x gradW(x_i - x_j);
-// |w_i| goes to .w for the vorticity pass
+// writes (w_i, |w_i|) and (v_i, |w_i|): the vorticity pass then gathers two
+// float4s per neighbour (x_j and v_j with |w_j|) instead of three
 // ---------------------------------------------------------------------------
 template <int L, int V>
 __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
                                               const int* __restrict__ nbr, const int* __restrict__ ncnt,
-                                              float4* __restrict__ omega) {
+                                              float4* __restrict__ omega, float4* __restrict__ vw) {
     using T = vec_t<V>;
     constexpr int P = L * V, B = batches<V>();
     const Team<L> tm = team_of<L>();
@@ -530,7 +493,11 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
         }
     }
     const f3 w3 = team_sum3<L>(fold3(wsum), tm.mask);
-    if (tm.t == 0) omega[k] = make_float4(w3.x, w3.y, w3.z, __fsqrt_rn(dot_fma(w3, w3)));
+    if (tm.t == 0) {
+        const float wl = __fsqrt_rn(dot_fma(w3, w3));
+        omega[k] = make_float4(w3.x, w3.y, w3.z, wl);
+        vw[k] = make_float4(vk.x, vk.y, vk.z, wl);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -539,32 +506,31 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
 // also writes the substep's final state (x, v, perm) for the next substep
 // ---------------------------------------------------------------------------
 template <bool DEBUG, int L, int V>
-__global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
+__global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restrict__ x, const float4* __restrict__ vw,
                                               const float4* __restrict__ omega, const int* __restrict__ nbr,
                                               const int* __restrict__ ncnt, float4* __restrict__ xout,
                                               float4* __restrict__ vout, const int* __restrict__ perm_in,
                                               int* __restrict__ perm_out, float4* __restrict__ vort_out,
                                               float4* __restrict__ visc_out) {
     using T = vec_t<V>;
-    constexpr int P = L * V, B = 2 / V;  // three 16-byte gathers per entry
+    constexpr int P = L * V, B = batches<V>();  // two 16-byte gathers per entry
     const Team<L> tm = team_of<L>();
     const int k = tm.k;
     if (k >= p.n) return;  // uniform over the team
     const f3 xk = make3(x[k]);
-    const f3 vk = make3(v[k]);
+    const f3 vk = make3(vw[k]);
     const int cnt = ncnt[k];
     T3<T> pv = zero3<T>(), eta = zero3<T>();
     for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
         int jj[B][V];
         load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
-        float4 xj[B][V], vj[B][V], oj[B][V];
+        float4 xj[B][V], vj[B][V];
 #pragma unroll
         for (int u = 0; u < B; ++u)
 #pragma unroll
             for (int c = 0; c < V; ++c) {
                 xj[u][c] = x[jj[u][c]];
-                vj[u][c] = v[jj[u][c]];
-                oj[u][c] = omega[jj[u][c]];
+                vj[u][c] = vw[jj[u][c]];
             }
 #pragma unroll
         for (int u = 0; u < B; ++u) {
@@ -576,7 +542,7 @@ __global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restric
             const T3<T> vv = pack3(vj[u]);
             const T3<T> vji = {vsub(vv.x, bc<T>(vk.x)), vsub(vv.y, bc<T>(vk.y)), vsub(vv.z, bc<T>(vk.z))};
             pv = {vfma(vji.x, w, pv.x), vfma(vji.y, w, pv.y), vfma(vji.z, w, pv.z)};
-            const T wl = packw(oj[u]);  // |w_j| (k_curl)
+            const T wl = packw(vj[u]);  // |w_j| (k_curl)
             eta = {vfma(wl, g.x, eta.x), vfma(wl, g.y, eta.y), vfma(wl, g.z, eta.z)};
         }
     }
@@ -647,24 +613,24 @@ void launch_features(const KParams& p, const float4* x, const float4* v, const i
 }
 
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
-                 cudaStream_t st) {
+                 float4* vw, cudaStream_t st) {
     with_lanes(p.lanes, [&](auto c) {
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
-        k_curl<L, V><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, omega);
+        k_curl<L, V><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, omega, vw);
     });
 }
 
-void launch_vort(const KParams& p, bool debug, const float4* x, const float4* v, const float4* omega, const int* nbr,
+void launch_vort(const KParams& p, bool debug, const float4* x, const float4* vw, const float4* omega, const int* nbr,
                  const int* ncnt, float4* xout, float4* vout, const int* perm_in, int* perm_out, float4* vort,
                  float4* visc, cudaStream_t st) {
     with_lanes(p.lanes, [&](auto c) {
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
         const int b = team_blocks(p.n, L, p.block);
         if (debug)
-            k_vort<true, L, V><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort,
+            k_vort<true, L, V><<<b, p.block, 0, st>>>(p, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort,
                                                       visc);
         else
-            k_vort<false, L, V><<<b, p.block, 0, st>>>(p, x, v, omega, nbr, ncnt, xout, vout, perm_in, perm_out,
+            k_vort<false, L, V><<<b, p.block, 0, st>>>(p, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out,
                                                        vort, visc);
     });
 }
