@@ -12,6 +12,7 @@
 
 #include "pbf_device.cuh"
 #include "pbf_mlp.h"
+#include "pbf_packed.cuh"
 #include "pbf_tc.cuh"
 
 namespace pbf {
@@ -105,6 +106,14 @@ __device__ __forceinline__ float gelu(float z) {
     return 0.5f * z * (1.0f + tanh_fast(u));
 }
 
+// GELU of two values with packed FP32 arithmetic (same expression order)
+__device__ __forceinline__ float2 gelu2(float2 z) {
+    const float2 z3 = vmul(vmul(vmul(bc<float2>(GELU_A), z), z), z);
+    const float2 u = vmul(bc<float2>(GELU_C), vadd(z, z3));
+    const float2 t = make_float2(tanh_fast(u.x), tanh_fast(u.y));
+    return vmul(vmul(bc<float2>(0.5f), z), vadd(bc<float2>(1.0f), t));
+}
+
 __device__ __forceinline__ float gelu_grad(float z) {
     const float u = GELU_C * (z + GELU_A * z * z * z);
     const float t = tanh_fast(u);
@@ -141,7 +150,10 @@ __device__ __forceinline__ float bf16_val(uint16_t b) { return __bfloat162float(
 __device__ __forceinline__ void put_row64(uint8_t* s, int row, const float (&v)[16], int c0) {
     uint32_t pk[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) pk[i] = (uint32_t)bf16_bits(v[2 * i]) | ((uint32_t)bf16_bits(v[2 * i + 1]) << 16);
+    for (int i = 0; i < 8; ++i) {
+        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);  // one packed conversion
+        pk[i] = *reinterpret_cast<const uint32_t*>(&b2);
+    }
     *reinterpret_cast<uint4*>(s + kmajor_offset(row, c0, 128)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     *reinterpret_cast<uint4*>(s + kmajor_offset(row, c0 + 8, 128)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
 }
@@ -265,10 +277,13 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
             tmem_wait_ld();
             float g[16];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const float z = v[i] + sb[B1_OFF + 16 * c + i];
-                v[i] = gelu(z);
-                g[i] = TRAIN ? gelu_grad(z) : 0.0f;
+            for (int i = 0; i < 16; i += 2) {
+                const float2 z = vadd(make_float2(v[i], v[i + 1]), make_float2(sb[B1_OFF + 16 * c + i], sb[B1_OFF + 16 * c + i + 1]));
+                g[i] = TRAIN ? gelu_grad(z.x) : 0.0f;
+                g[i + 1] = TRAIN ? gelu_grad(z.y) : 0.0f;
+                const float2 hh = gelu2(z);
+                v[i] = hh.x;
+                v[i + 1] = hh.y;
             }
             put_row64(smem + FWD_SH1, t, v, 16 * c);
             if (TRAIN && valid) {
@@ -293,10 +308,13 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
             tmem_wait_ld();
             float g[16];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const float z = v[i] + sb[B2_OFF + 16 * c + i];
-                v[i] = gelu(z);
-                g[i] = TRAIN ? gelu_grad(z) : 0.0f;
+            for (int i = 0; i < 16; i += 2) {
+                const float2 z = vadd(make_float2(v[i], v[i + 1]), make_float2(sb[B2_OFF + 16 * c + i], sb[B2_OFF + 16 * c + i + 1]));
+                g[i] = TRAIN ? gelu_grad(z.x) : 0.0f;
+                g[i + 1] = TRAIN ? gelu_grad(z.y) : 0.0f;
+                const float2 hh = gelu2(z);
+                v[i] = hh.x;
+                v[i + 1] = hh.y;
             }
             put_row64(smem + FWD_SH2, t, v, 16 * c);
             if (TRAIN && valid) {
@@ -322,10 +340,18 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
             float v[16];
             tmem_ld16(lane_base + 16 * c, v);
             tmem_wait_ld();
+            float hs[16];
+#pragma unroll
+            for (int i = 0; i < 16; i += 2) {
+                const float2 hh = gelu2(vadd(make_float2(v[i], v[i + 1]),
+                                             make_float2(sb[B3_OFF + 16 * c + i], sb[B3_OFF + 16 * c + i + 1])));
+                hs[i] = hh.x;
+                hs[i + 1] = hh.y;
+            }
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const float z = v[i] + sb[B3_OFF + 16 * c + i];
-                const float h = gelu(z);
+                const float h = hs[i];
                 y = __fmaf_rn(h, sw4[16 * c + i], y);
                 if (TRAIN) {
                     h3f[16 * c + i] = h;
