@@ -130,8 +130,6 @@ def collect(scene, substeps: int, rows_per_substep: int, seed: int = 0, warmup: 
     """Runs the plain solver on `scene` and gathers `rows_per_substep` random
     particles' (features, total lambda) after every substep. Returns device
     tensors feat [S, 12], target [S]."""
-    import torch
-
     from .solver import Solver
     kw = dict(ext or {})
     kw["record_features"] = 1
@@ -139,6 +137,31 @@ def collect(scene, substeps: int, rows_per_substep: int, seed: int = 0, warmup: 
     s.upload(scene.pos, scene.vel)
     if warmup:
         s.step(warmup)
+    try:
+        return collect_from(s, substeps, rows_per_substep, seed)
+    finally:
+        s.close()
+
+
+def collect_batch(scenes_, substeps: int, rows_per_substep: int, seed: int = 0, ext: Optional[dict] = None):
+    """collect() on a batch of scenes (pbf_b200.scenes.batch_inputs) run as one BatchSolver."""
+    from . import scenes as S
+    from .solver import BatchSolver
+    para, descs, ov, pos, vel = S.batch_inputs(scenes_)
+    ov.update(ext or {})
+    ov["record_features"] = 1
+    b = BatchSolver(para, descs, S.default_ext(**ov))
+    b.upload(pos, vel)
+    try:
+        return collect_from(b, substeps, rows_per_substep, seed)
+    finally:
+        b.close()
+
+
+def collect_from(s, substeps: int, rows_per_substep: int, seed: int = 0):
+    """Steps an uploaded solver created with record_features = 1 and gathers
+    `rows_per_substep` random particles' (features, total lambda) after every substep."""
+    import torch
     g = torch.Generator(device="cuda").manual_seed(seed)
     total = substeps * rows_per_substep
     feat = torch.empty((total, 12), dtype=torch.float32, device="cuda")
@@ -151,7 +174,6 @@ def collect(scene, substeps: int, rows_per_substep: int, seed: int = 0, warmup: 
         check(lib().pbf_gather_training_rows(s.handle, slots.data_ptr(), rows_per_substep, feat[a:b].data_ptr(),
                                              target[a:b].data_ptr(), int(stream.cuda_stream)))
     torch.cuda.synchronize()
-    s.close()
     return feat, target
 
 

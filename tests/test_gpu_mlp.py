@@ -174,3 +174,15 @@ def test_warm_start_beats_the_same_iterations_without_it():
     print(f"losses {losses[0][1]:.4g} -> {losses[-1][1]:.4g}; mean density error: plain x2 {plain2[1]:.5f}, "
           f"warm+1 {warm2[1]:.5f}; max: {plain2[0]:.4f} vs {warm2[0]:.4f}")
     assert warm2[1] < plain2[1]
+
+
+def test_collect_batch_rows():
+    """Training rows gathered from a batch of scenes: finite features, the
+    neighbour fraction in [0, 1], and a non-trivial total lambda."""
+    scs = scenes.config2(seed=3, n_scenes=3, lo=300, hi=1500, iterations=3)
+    feat, target = learned.collect_batch(scs, substeps=4, rows_per_substep=64, seed=1)
+    f, t = feat.cpu().numpy(), target.cpu().numpy()
+    assert f.shape == (256, 12) and t.shape == (256,)
+    assert np.isfinite(f).all() and np.isfinite(t).all()
+    assert (f[:, 0] >= 0).all() and (f[:, 0] <= 1).all()
+    assert np.abs(t).max() > 0
