@@ -208,7 +208,9 @@ int pbf_get_layout(const pbf_solver* s, int* ncells, int* stride, int* max_neigh
 int pbf_stage_times(pbf_solver* s, float* ms, int nstages);
 
 /* Number of kernel launches in one substep (kernel nodes of the substep graph);
- * negative status on error. */
+ * negative status on error. With ext.adaptive (and ext.profile off) the
+ * corrections run in a device-side loop (a graph while node): its body's
+ * kernels count once here and launch once per pass. */
 int pbf_graph_kernel_count(pbf_solver* s);
 
 /* One-sided density error max_i max(rho_i/rho0 - 1, 0) and its mean over the

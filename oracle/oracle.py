@@ -52,6 +52,7 @@ def olib() -> C.CDLL:
         L.oracle_create.restype = C.c_void_p
         L.oracle_create.argtypes = [C.POINTER(OracleParams), C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.oracle_substep.argtypes = [C.c_void_p]
+        L.oracle_substep_adaptive.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
         L.oracle_build_only.argtypes = [C.c_void_p]
         L.oracle_get.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.oracle_ncells.argtypes = [C.c_void_p]
@@ -131,6 +132,12 @@ class Oracle:
     def substep(self, count: int = 1) -> None:
         for _ in range(count):
             olib().oracle_substep(self._h)
+
+    def substep_adaptive(self, tol: float, min_iterations: int, max_iterations: int) -> int:
+        """One adaptive substep of the CUDA library (ext.adaptive): corrections until
+        the lambda pass measures a max one-sided density error <= tol, at least
+        min_iterations (>= 1) and at most max_iterations; returns the count."""
+        return int(olib().oracle_substep_adaptive(self._h, float(tol), int(min_iterations), int(max_iterations)))
 
     def build_only(self) -> None:
         olib().oracle_build_only(self._h)

@@ -560,9 +560,12 @@ public:
         return std::min(p.lanes, kMaxLanes);
     }
 
+    T err_max = 0;  // max one-sided density error seen by the last compute_lambda
+
     void compute_lambda() {
         // calculateLambda cu:156-180; CPU src/solver.cpp:78-95
         const int L = lanes();
+        err_max = 0;
         for (int i = 0; i < n; ++i) {
             T rl[kMaxLanes], gml[kMaxLanes];
             V3<T> gsl[kMaxLanes];
@@ -587,6 +590,8 @@ public:
             }
             T r = combine_lanes(rl, L), gm = combine_lanes(gml, L);
             V3<T> gs = combine_lanes(gsl, L);
+            // one-sided error of the fluid density (before any wall term)
+            err_max = std::max(err_max, std::max(r / k.rho0 - (T)1, (T)0));
             if (p.flags & ORACLE_WALL_DENSITY) {
                 V3<T> gw;
                 r = r + wall_term(x[i], gw);
@@ -753,6 +758,27 @@ public:
         }
         vorticity_viscosity();
     }
+
+    // The CUDA library's adaptive substep (no reference counterpart): Jacobi
+    // corrections until the max one-sided density error measured by the lambda
+    // pass is <= tol, at least min_it and at most max_it corrections; the
+    // velocity then comes from the total displacement. Returns the corrections.
+    int substep_adaptive(double tol, int min_it, int max_it) {
+        predict();
+        build_grid();
+        build_neighbors();
+        int it = 0;
+        for (; it < max_it; ++it) {
+            compute_lambda();
+            if (it >= min_it && (double)err_max <= tol) break;
+            compute_dp();
+            update_positions(false);
+        }
+        for (int i = 0; i < n; ++i)
+            v[i] = {(x[i].x - xold[i].x) / k.dt, (x[i].y - xold[i].y) / k.dt, (x[i].z - xold[i].z) / k.dt};
+        vorticity_viscosity();
+        return it;
+    }
 };
 
 struct Handle {
@@ -823,6 +849,12 @@ int oracle_substep(void* hv) {
     if (!h) return -1;
     if (h->f) h->f->substep(); else h->d->substep();
     return 0;
+}
+
+int oracle_substep_adaptive(void* hv, double tol, int min_it, int max_it) {
+    Handle* h = (Handle*)hv;
+    if (!h) return -1;
+    return h->f ? h->f->substep_adaptive(tol, min_it, max_it) : h->d->substep_adaptive(tol, min_it, max_it);
 }
 
 // Runs only the grid build (hash, count, scan, sort) and neighbour search on the

@@ -60,7 +60,7 @@ struct DevStats {
     int done;
     int iters;
     int conv_slot;
-    int pad;
+    int loop_k;  // passes of the device-side correction loop
     // not reset per substep:
     int err;
     int fallback;
@@ -109,9 +109,11 @@ struct pbf_solver {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t cap_stream = nullptr;
+    cudaStream_t body_stream = nullptr;  // captures the body of the device-side correction loop
     cudaStream_t last_stream = nullptr;
     std::vector<StageEvents> prof;  // event pairs captured around each launch (ext.profile)
     int kernel_nodes = 0;
+    int loop_kernel_nodes = 0;  // kernels of one pass of the device-side correction loop
     bool uploaded = false;
     long long substeps = 0, total_iters = 0, fallbacks = 0;
 };
@@ -202,6 +204,7 @@ void free_all(pbf_solver* s) {
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
     if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+    if (s->body_stream) cudaStreamDestroy(s->body_stream);
     for (auto& e : s->prof) {
         cudaEventDestroy(e.a);
         cudaEventDestroy(e.b);
@@ -280,8 +283,66 @@ struct Prof {
     }
 };
 
+int count_kernel_nodes(cudaGraph_t g, int* out) {
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+    int k = 0;
+    for (auto nd : nodes) {
+        // this runtime cannot name the type of a conditional node under newer
+        // drivers (it returns cudaErrorUnknown); such a node is not a kernel
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess) {
+            if (t == cudaGraphNodeTypeKernel) ++k;
+        } else {
+            cudaGetLastError();
+        }
+    }
+    *out = k;
+    return PBF_OK;
+}
+
+// Appends to the capture on `st` the adaptive correction loop as a graph while
+// node. Each pass runs one correction (lambda, then delta-p, which ends the loop
+// instead when the lambda pass measured an error within tolerance) and the
+// loop-control kernel; passes run for slots first, first + 1, ... < max_it.
+// A converged substep therefore launches no further kernels.
+int capture_correction_loop(pbf_solver* s, cudaStream_t st, int first, int min_it, int max_it, float* acc, bool dbg) {
+    const KParams& kp = s->kp;
+    DevStats* ds = s->dstats;
+    cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* dp = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &dp, &nd));
+    if (status != cudaStreamCaptureStatusActive) return fail(PBF_ERR_CUDA, "correction loop: stream is not capturing");
+    const std::vector<cudaGraphNode_t> deps(dp, dp + nd);
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, first < max_it ? 1u : 0u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps.data(), deps.size(), &np));
+    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    cudaStream_t bs = s->body_stream;
+    CK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const IterCtl c{&ds->done, ds->max_bits, ds->sum, &ds->iters, &ds->conv_slot, (double)s->ext.density_tol,
+                    first, min_it, &ds->loop_k, acc};
+    launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, c, bs);
+    launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, nullptr, s->dp_dbg, c, bs);
+    launch_loop_ctl(h, &ds->loop_k, &ds->done, first, max_it, bs);
+    cudaGraph_t out = nullptr;
+    CK(cudaStreamEndCapture(bs, &out));
+    return count_kernel_nodes(body, &s->loop_kernel_nodes);
+}
+
 // Enqueue one substep on `st` (captured into the graph).
-void enqueue_substep(pbf_solver* s, cudaStream_t st) {
+int enqueue_substep(pbf_solver* s, cudaStream_t st) {
     const KParams& kp = s->kp;
     const bool dbg = s->ext.debug != 0;
     const int n = s->n;
@@ -344,16 +405,25 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
             });
     } else {
         // Iterate until the max density error is within tolerance (slot k holds
-        // the error after k corrections). The graph holds max_iterations
-        // iterations; once converged the rest return at once. Corrections beyond
-        // the configured count are the plain-iteration fallback.
+        // the error after k corrections), at least the configured count and at
+        // most max_iterations. Corrections beyond the configured count are the
+        // plain-iteration fallback.
         const int min_it = std::max(iters, 1);
         const int max_it = s->ext.max_iterations;
-        for (int it = first; it < max_it; ++it) {
-            const IterCtl c{&ds->done, &ds->max_bits[it], &ds->sum[it], &ds->iters, &ds->conv_slot,
-                            (double)s->ext.density_tol, it, it >= min_it ? 1 : 0, acc};
-            P(ST_LAMBDA, [&] { launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, c, st); });
-            P(ST_DP, [&] { launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, nullptr, s->dp_dbg, c, st); });
+        if (!P.on) {
+            const int rc = capture_correction_loop(s, st, first, min_it, max_it, acc, dbg);
+            if (rc) return rc;
+        } else {
+            // Profiled (event records cannot sit in a loop body): the graph holds
+            // max_iterations iterations; once converged the rest return at once.
+            for (int it = first; it < max_it; ++it) {
+                const IterCtl c{&ds->done, ds->max_bits, ds->sum, &ds->iters, &ds->conv_slot,
+                                (double)s->ext.density_tol, it, min_it, nullptr, acc};
+                P(ST_LAMBDA, [&] { launch_lambda(kp, dbg, s->Px, s->nbr, s->ncnt, s->Q, s->rho_dbg, c, st); });
+                P(ST_DP, [&] {
+                    launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, nullptr, s->dp_dbg, c, st);
+                });
+            }
         }
         // error after the last correction, for substeps that reached the cap
         P(ST_MEASURE, [&] {
@@ -367,6 +437,7 @@ void enqueue_substep(pbf_solver* s, cudaStream_t st) {
         launch_vort(kp, dbg, s->Px, s->vw, s->omega, s->nbr, s->ncnt, s->Sx, s->Sv, s->Pperm, s->Sperm,
                     s->vort_dbg, s->visc_dbg, st);
     });
+    return PBF_OK;
 }
 
 int build_graph(pbf_solver* s) {
@@ -383,21 +454,21 @@ int build_graph(pbf_solver* s) {
         cudaEventDestroy(e.b);
     }
     s->prof.clear();
+    s->loop_kernel_nodes = 0;
     CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_substep(s, s->cap_stream);
+    const int rc = enqueue_substep(s, s->cap_stream);
     cudaError_t e = cudaStreamEndCapture(s->cap_stream, &s->graph);
+    if (rc) {
+        if (s->graph) cudaGraphDestroy(s->graph);
+        s->graph = nullptr;
+        return rc;
+    }
     if (e != cudaSuccess) return fail(PBF_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
     CK(cudaGraphInstantiate(&s->exec, s->graph, 0));
-    size_t nn = 0;
-    CK(cudaGraphGetNodes(s->graph, nullptr, &nn));
-    std::vector<cudaGraphNode_t> nodes(nn);
-    CK(cudaGraphGetNodes(s->graph, nodes.data(), &nn));
-    s->kernel_nodes = 0;
-    for (auto nd : nodes) {
-        cudaGraphNodeType t;
-        CK(cudaGraphNodeGetType(nd, &t));
-        if (t == cudaGraphNodeTypeKernel) ++s->kernel_nodes;
-    }
+    int top = 0;
+    const int rc2 = count_kernel_nodes(s->graph, &top);
+    if (rc2) return rc2;
+    s->kernel_nodes = top + s->loop_kernel_nodes;
     return PBF_OK;
 }
 
@@ -590,6 +661,7 @@ int create_common(const pbf_solver_parameter* para, int nscenes, const pbf_scene
     if (e == cudaSuccess) e = cudaMemset(s->lam_acc, 0, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaMemset(s->lam0, 0, sizeof(float) * n);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         free_all(s);
         delete s;

@@ -87,15 +87,17 @@ struct KParams {
 // when that error is within tol. done == nullptr: fixed iteration count.
 struct IterCtl {
     int* done;
-    unsigned long long* max_bits;  // slot: max error as ordered double bits
-    double* sum;                   // slot: sum of errors
+    unsigned long long* max_bits;  // per-slot max error as ordered double bits (slot k: after k corrections)
+    double* sum;                   // per-slot sum of errors
     int* iters;                    // corrections applied
     int* conv_slot;                // slot whose error met the tolerance
     double tol;
-    int slot;
-    int may_stop;                  // 0 while below the minimum iteration count
+    int slot;                      // this pass's slot; plus *loop_k when loop_k is set
+    int min_slot;                  // the loop may end at slots >= min_slot
+    const int* loop_k;             // pass counter of a device-side loop (graph while node), or null
     float* lam_acc;                // when set, the lambda pass adds its lambda here (the
                                    // substep's total lambda: warm-start feature and target)
+    __device__ __forceinline__ int cur_slot() const { return loop_k ? slot + *loop_k : slot; }
 };
 
 // ---- deterministic sine ------------------------------------------------------

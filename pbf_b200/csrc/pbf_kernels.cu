@@ -428,6 +428,16 @@ __global__ void k_count_fallback(const int* __restrict__ iters, int first, int c
     *total += used;
 }
 
+// Control of the device-side correction loop (a graph while node whose body is
+// one lambda pass and one delta-p pass, then this kernel): counts the pass and
+// keeps the loop running while the error is above tolerance and slots are left.
+__global__ void k_loop_ctl(cudaGraphConditionalHandle h, int* __restrict__ loop_k, const int* __restrict__ done,
+                           int first, int max_it) {
+    const int k = *loop_k + 1;
+    *loop_k = k;
+    cudaGraphSetConditional(h, (*done == 0 && first + k < max_it) ? 1u : 0u);
+}
+
 // v = (x - x_old) / dt as its own pass (adaptive iteration counts)
 __global__ void __launch_bounds__(256) k_velocity(KParams p, const float4* __restrict__ x,
                                                   const float4* __restrict__ xold, float4* __restrict__ v) {
@@ -593,6 +603,11 @@ void launch_gather_rows(const int* slots, int count, int n, const float* feat, c
 void launch_count_fallback(const int* iters, int first, int configured, int* fallback, long long* total,
                            cudaStream_t st) {
     k_count_fallback<<<1, 1, 0, st>>>(iters, first, configured, fallback, total);
+}
+
+void launch_loop_ctl(cudaGraphConditionalHandle h, int* loop_k, const int* done, int first, int max_it,
+                     cudaStream_t st) {
+    k_loop_ctl<<<1, 1, 0, st>>>(h, loop_k, done, first, max_it);
 }
 
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st) {

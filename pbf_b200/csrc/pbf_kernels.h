@@ -33,6 +33,8 @@ void launch_gather_rows(const int* slots, int count, int n, const float* feat, c
                         float* out_target, int* err, cudaStream_t st);
 void launch_count_fallback(const int* iters, int first, int configured, int* fallback, long long* total,
                            cudaStream_t st);
+void launch_loop_ctl(cudaGraphConditionalHandle h, int* loop_k, const int* done, int first, int max_it,
+                     cudaStream_t st);
 void launch_velocity(const KParams& p, const float4* x, const float4* xold, float4* v, cudaStream_t st);
 // Curl: omega = (w, |w|) and vw = (v, |w|) per particle.
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,

@@ -259,7 +259,10 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_lambda(KParams p, const
             if (DEBUG) rho_out[k] = rhos;
         }
     }
-    if (ctl.max_bits) block_error_reduce(err, ctl.max_bits, ctl.sum);
+    if (ctl.max_bits) {
+        const int sl = ctl.cur_slot();
+        block_error_reduce(err, ctl.max_bits + sl, ctl.sum + sl);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -394,10 +397,11 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_dp(KParams p, const flo
         if (*ctl.done) return;
         // the lambda pass just measured the positions this pass would correct;
         // when they are within tolerance the loop ends here
-        if (ctl.may_stop && __longlong_as_double((long long)*ctl.max_bits) <= ctl.tol) {
+        const int sl = ctl.cur_slot();
+        if (sl >= ctl.min_slot && __longlong_as_double((long long)ctl.max_bits[sl]) <= ctl.tol) {
             if (blockIdx.x == 0 && threadIdx.x == 0) {
                 *ctl.done = 1;
-                *ctl.conv_slot = ctl.slot;
+                *ctl.conv_slot = sl;
             }
             return;
         }

@@ -258,6 +258,28 @@ def test_adaptive_iterations_reach_tolerance():
     assert mx <= 0.005 + 1e-4 or st["last_iterations"] == 12
 
 
+@pytest.mark.parametrize("profile", [0, 1])
+def test_adaptive_loop_bitexact(profile):
+    """The adaptive corrections (a device-side graph while loop; unrolled when
+    profiling) against the oracle's adaptive substep: the same correction count
+    every substep and bit-identical state."""
+    sc = scenes.dam_break(16, (40, 20, 20), stable=True, iterations=1)
+    s, orc = make_pair(sc, adaptive=1, density_tol=0.005, max_iterations=12, profile=profile)
+    tol = float(np.float32(0.005))
+    counts = []
+    for _ in range(4):
+        s.step(1)
+        want = orc.substep_adaptive(tol, 1, 12)
+        counts.append(want)
+        assert s.stats()["last_iterations"] == want
+        assert_state_bitexact(s, orc)
+    assert max(counts) > 1  # the tolerance made the loop run more than once
+    plain = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(adaptive=1, density_tol=0.005, max_iterations=12,
+                                                               profile=1 - profile))
+    if profile == 0:  # one pass of the loop body counts once
+        assert s.kernel_count() < plain.kernel_count()
+
+
 def test_host_errors():
     sc = scenes.dam_break(4, (40, 20, 20))
     with pytest.raises(PBFError) as e:

@@ -177,3 +177,24 @@ def test_soft_rsqrt_within_two_ulp():
         exact = 1.0 / math.sqrt(float(x))
         worst = max(worst, abs(float(y) - exact) / float(np.spacing(np.float32(exact))))
     assert worst <= 2.0, worst
+
+
+def test_oracle_adaptive_substep_limits():
+    """The adaptive substep at its two limits: a tolerance every state meets runs
+    exactly the minimum count and equals the plain substep with that count; a
+    zero tolerance runs to the cap. In between, the count lies between them and
+    the lambda pass of the last correction measured an error above tolerance."""
+    sc = scenes.dam_break(16, (40, 20, 20), stable=True, iterations=3)
+    prm = O.params_for_scene(sc)
+    plain = O.Oracle(prm, sc.pos, sc.vel)
+    loose = O.Oracle(prm, sc.pos, sc.vel)
+    tight = O.Oracle(prm, sc.pos, sc.vel)
+    mid = O.Oracle(prm, sc.pos, sc.vel)
+    for _ in range(2):
+        plain.substep()
+        assert loose.substep_adaptive(1e30, 3, 12) == 3
+        assert tight.substep_adaptive(0.0, 1, 5) == 5
+        assert 1 <= mid.substep_adaptive(float(np.float32(0.003)), 1, 12) <= 12
+    for name in ("x", "v", "curl", "vort"):  # (lambda differs: the adaptive loop measures once more)
+        assert np.array_equal(plain.get(name), loose.get(name)), name
+    assert not np.array_equal(plain.get("x"), tight.get("x"))
