@@ -214,14 +214,16 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_lambda(KParams p, const
         const int cnt = ncnt[k];
         T rho = bc<T>(0.0f), gm = bc<T>(0.0f);
         T3<T> gs = zero3<T>();
+        int jj[B][V];
+        load_idx<V, P, B>(p, nbr, k, V * tm.t, cnt, jj);
         for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
-            int jj[B][V];
-            load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
             float4 xj[B][V];
 #pragma unroll
             for (int u = 0; u < B; ++u)
 #pragma unroll
                 for (int v = 0; v < V; ++v) xj[u][v] = x[jj[u][v]];
+            // the next batch's indices load while this batch computes
+            load_idx<V, P, B>(p, nbr, k, q0 + P * B, cnt, jj);
 #pragma unroll
             for (int u = 0; u < B; ++u) {
                 const int q = q0 + u * P;
@@ -298,9 +300,9 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
     T rho = bc<T>(0.0f), gm = bc<T>(0.0f), div = bc<T>(0.0f), close = bc<T>(0.0f), dv2 = bc<T>(0.0f);
     T3<T> gs = zero3<T>(), rs = zero3<T>();
     const float q2 = 0.25f * p.h2;
+    int jj[B][V];
+    load_idx<V, P, B>(p, nbr, k, V * tm.t, cnt, jj);
     for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
-        int jj[B][V];
-        load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
         float4 xj[B][V], vj[B][V];
 #pragma unroll
         for (int u = 0; u < B; ++u)
@@ -309,6 +311,8 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
                 xj[u][c] = x[jj[u][c]];
                 vj[u][c] = v[jj[u][c]];
             }
+        // the next batch's indices load while this batch computes
+        load_idx<V, P, B>(p, nbr, k, q0 + P * B, cnt, jj);
 #pragma unroll
         for (int u = 0; u < B; ++u) {
             const int q = q0 + u * P;
@@ -415,14 +419,19 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_dp(KParams p, const flo
     const float lk = xk4.w;
     const int cnt = ncnt[k];
     T3<T> a = zero3<T>();
+    // index prefetch one batch ahead (packed form only: the scalar form has no
+    // registers left for it within 40)
+    constexpr bool PF = V == 2;
+    int jj[B][V];
+    if (PF) load_idx<V, P, B>(p, nbr, k, V * tm.t, cnt, jj);
     for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
-        int jj[B][V];
-        load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
+        if (!PF) load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
         float4 xj[B][V];
 #pragma unroll
         for (int u = 0; u < B; ++u)
 #pragma unroll
             for (int c = 0; c < V; ++c) xj[u][c] = xl[jj[u][c]];
+        if (PF) load_idx<V, P, B>(p, nbr, k, q0 + P * B, cnt, jj);
 #pragma unroll
         for (int u = 0; u < B; ++u) {
             const int q = q0 + u * P;
@@ -473,9 +482,9 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
     const f3 vk = make3(v[k]);
     const int cnt = ncnt[k];
     T3<T> wsum = zero3<T>();
+    int jj[B][V];
+    load_idx<V, P, B>(p, nbr, k, V * tm.t, cnt, jj);
     for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
-        int jj[B][V];
-        load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
         float4 xj[B][V], vj[B][V];
 #pragma unroll
         for (int u = 0; u < B; ++u)
@@ -484,6 +493,8 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
                 xj[u][c] = x[jj[u][c]];
                 vj[u][c] = v[jj[u][c]];
             }
+        // the next batch's indices load while this batch computes
+        load_idx<V, P, B>(p, nbr, k, q0 + P * B, cnt, jj);
 #pragma unroll
         for (int u = 0; u < B; ++u) {
             const int q = q0 + u * P;
@@ -525,6 +536,8 @@ __global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restric
     const f3 vk = make3(vw[k]);
     const int cnt = ncnt[k];
     T3<T> pv = zero3<T>(), eta = zero3<T>();
+    // (no index prefetch here: the three gathers per entry leave no registers
+    // for it within 64)
     for (int q0 = V * tm.t; q0 < cnt; q0 += P * B) {
         int jj[B][V];
         load_idx<V, P, B>(p, nbr, k, q0, cnt, jj);
