@@ -177,6 +177,20 @@ int pbf_bind_position(pbf_solver* s, float* d_pos);
  * the captured substep graph `substeps` times on `stream`. */
 int pbf_step(pbf_solver* s, int substeps, void* stream);
 
+/* One frame from and to host memory, asynchronous and pipelined across calls
+ * (no reference counterpart; the host side of initCUDASolverDataBuffer's
+ * copies and cudaPBFSolve in one call): copies pos and vel (AoS xyz float[3n];
+ * page-locked memory lets the copies overlap) to the device on an internal
+ * stream, uploads them as pbf_upload_device does and runs `substeps` substeps
+ * on `stream`, then copies the positions (original order) to pos_out on a
+ * second internal stream. Device staging is double-buffered, so the copies of
+ * neighbouring calls overlap the substeps. The three host buffers must stay
+ * untouched until the call's copies are done: pbf_host_fence(s, stream) makes
+ * `stream` wait for every copy issued so far; synchronise that stream before
+ * reading pos_out. */
+int pbf_step_host(pbf_solver* s, const float* pos, const float* vel, float* pos_out, int substeps, void* stream);
+int pbf_host_fence(pbf_solver* s, void* stream);
+
 /* Host copies of positions / velocities in original order (either may be NULL). */
 int pbf_download(pbf_solver* s, float* pos, float* vel);
 

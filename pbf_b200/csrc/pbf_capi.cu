@@ -78,6 +78,16 @@ struct StageEvents {
 
 }  // namespace
 
+// Double-buffered staging of pbf_step_host: host copies run on their own
+// streams, ordered against the solver's stream by events.
+struct HostPipe {
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    float* in[2] = {nullptr, nullptr};   // pos, vel: float[6n]
+    float* out[2] = {nullptr, nullptr};  // positions: float[3n]
+    cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
+    long long calls = 0;
+};
+
 struct pbf_solver {
     pbf_solver_parameter para{};
     pbf_ext_params ext{};
@@ -116,6 +126,7 @@ struct pbf_solver {
     int loop_kernel_nodes = 0;  // kernels of one pass of the device-side correction loop
     bool uploaded = false;
     long long substeps = 0, total_iters = 0, fallbacks = 0;
+    HostPipe* hp = nullptr;  // pbf_step_host staging, created on first use
 };
 
 namespace {
@@ -204,6 +215,18 @@ void free_all(pbf_solver* s) {
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
     if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+    if (HostPipe* hp = s->hp) {
+        for (int b = 0; b < 2; ++b) {
+            if (hp->in[b]) cudaFree(hp->in[b]);
+            if (hp->out[b]) cudaFree(hp->out[b]);
+            for (cudaEvent_t e : {hp->in_ready[b], hp->in_free[b], hp->out_ready[b], hp->out_free[b]})
+                if (e) cudaEventDestroy(e);
+        }
+        if (hp->h2d) cudaStreamDestroy(hp->h2d);
+        if (hp->d2h) cudaStreamDestroy(hp->d2h);
+        delete hp;
+        s->hp = nullptr;
+    }
     if (s->body_stream) cudaStreamDestroy(s->body_stream);
     for (auto& e : s->prof) {
         cudaEventDestroy(e.a);
@@ -747,6 +770,60 @@ int pbf_step(pbf_solver* s, int substeps, void* stream) {
     }
     s->last_stream = st;
     s->substeps += substeps;
+    return PBF_OK;
+}
+
+int pbf_step_host(pbf_solver* s, const float* pos, const float* vel, float* pos_out, int substeps, void* stream) {
+    if (!s || !pos || !vel || !pos_out) return fail(PBF_ERR_INVALID, "null argument");
+    if (substeps < 0) return fail(PBF_ERR_INVALID, "negative substep count");
+    if (!s->hp) {
+        HostPipe* hp = new (std::nothrow) HostPipe();
+        if (!hp) return fail(PBF_ERR_ALLOC, "host allocation failed");
+        s->hp = hp;
+        const size_t n = s->n;
+        cudaError_t e = cudaStreamCreateWithFlags(&hp->h2d, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&hp->d2h, cudaStreamNonBlocking);
+        for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+            e = cudaMalloc(&hp->in[b], sizeof(float) * 6 * std::max<size_t>(n, 1));
+            if (e == cudaSuccess) e = cudaMalloc(&hp->out[b], sizeof(float) * 3 * std::max<size_t>(n, 1));
+            for (cudaEvent_t* ev : {&hp->in_ready[b], &hp->in_free[b], &hp->out_ready[b], &hp->out_free[b]})
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess) return fail(PBF_ERR_ALLOC, "pbf_step_host staging: %s", cudaGetErrorString(e));
+    }
+    HostPipe& hp = *s->hp;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int b = (int)(hp.calls & 1);
+    const size_t bytes = sizeof(float) * 3 * (size_t)s->n;
+    // inputs: into staging b once the upload of two calls ago has read it
+    CK(cudaStreamWaitEvent(hp.h2d, hp.in_free[b], 0));
+    CK(cudaMemcpyAsync(hp.in[b], pos, bytes, cudaMemcpyHostToDevice, hp.h2d));
+    CK(cudaMemcpyAsync(hp.in[b] + 3 * (size_t)s->n, vel, bytes, cudaMemcpyHostToDevice, hp.h2d));
+    CK(cudaEventRecord(hp.in_ready[b], hp.h2d));
+    CK(cudaStreamWaitEvent(st, hp.in_ready[b], 0));
+    int rc = pbf_upload_device(s, hp.in[b], hp.in[b] + 3 * (size_t)s->n, s->n, stream);
+    if (rc) return rc;
+    CK(cudaEventRecord(hp.in_free[b], st));
+    rc = pbf_step(s, substeps, stream);
+    if (rc) return rc;
+    // result: into staging b once the copy-out of two calls ago has read it
+    CK(cudaStreamWaitEvent(st, hp.out_free[b], 0));
+    rc = pbf_download_device(s, hp.out[b], nullptr, stream);
+    if (rc) return rc;
+    CK(cudaEventRecord(hp.out_ready[b], st));
+    CK(cudaStreamWaitEvent(hp.d2h, hp.out_ready[b], 0));
+    CK(cudaMemcpyAsync(pos_out, hp.out[b], bytes, cudaMemcpyDeviceToHost, hp.d2h));
+    CK(cudaEventRecord(hp.out_free[b], hp.d2h));
+    ++hp.calls;
+    return PBF_OK;
+}
+
+int pbf_host_fence(pbf_solver* s, void* stream) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (!s->hp || s->hp->calls == 0) return PBF_OK;
+    // copies of one direction complete in call order; the last copy-out comes
+    // after its call's copy-in
+    CK(cudaStreamWaitEvent((cudaStream_t)stream, s->hp->out_free[(s->hp->calls - 1) & 1], 0));
     return PBF_OK;
 }
 

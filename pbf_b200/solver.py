@@ -49,6 +49,19 @@ def _stream_handle(stream) -> Optional[int]:
     return int(stream.cuda_stream)  # torch.cuda.Stream
 
 
+def _host_ptr(a, n: int, writable: bool = False) -> int:
+    """Address of an n x 3 float32 C-contiguous host array (numpy or CPU tensor)."""
+    if hasattr(a, "data_ptr"):  # torch tensor
+        if a.is_cuda or a.dtype.itemsize != 4 or not a.is_contiguous() or a.numel() != 3 * n:
+            raise ValueError("expected a contiguous float32 host tensor of n x 3")
+        return a.data_ptr()
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous and a.size == 3 * n):
+        raise ValueError("expected a C-contiguous float32 array of n x 3")
+    if writable and not a.flags.writeable:
+        raise ValueError("output array is read-only")
+    return a.ctypes.data
+
+
 def _f6(b: Sequence[float]):
     a = (C.c_float * 6)(*[float(x) for x in b])
     return a
@@ -125,6 +138,19 @@ class Solver:
         pp = None if d_pos is None else (d_pos if isinstance(d_pos, int) else d_pos.data_ptr())
         vp = None if d_vel is None else (d_vel if isinstance(d_vel, int) else d_vel.data_ptr())
         check(lib().pbf_download_device(self._h, pp, vp, _stream_handle(stream)))
+
+    def step_host(self, pos, vel, pos_out, substeps: int = 1, stream=None) -> None:
+        """One asynchronous frame from and to host memory (pbf_step_host): pos, vel
+        and pos_out are n x 3 float32 host arrays (numpy or CPU tensors; pinned
+        memory lets the copies overlap). They must stay untouched until
+        host_fence(stream) has been called and the stream synchronised."""
+        check(lib().pbf_step_host(self._h, _host_ptr(pos, self.n), _host_ptr(vel, self.n),
+                                  _host_ptr(pos_out, self.n, writable=True), int(substeps),
+                                  _stream_handle(stream)))
+
+    def host_fence(self, stream=None) -> None:
+        """Makes `stream` wait for every copy issued by step_host so far."""
+        check(lib().pbf_host_fence(self._h, _stream_handle(stream)))
 
     def stats(self, raise_on_error: bool = True) -> dict:
         st = Stats()

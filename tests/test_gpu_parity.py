@@ -312,3 +312,32 @@ def test_drop_in_entry_points_and_bound_position():
         torch.cuda.synchronize()
         assert bits_equal(buf.cpu().numpy(), oracle_original(orc, "x").astype(np.float32))
     P.freeCUDASolverDataBuffer(data)
+
+
+def test_step_host_pipelined_frames():
+    """pbf_step_host: every call uploads its own host inputs, runs a substep and
+    copies the positions back; with double-buffered staging, interleaved calls on
+    two different states each give the positions of a plain upload, step and
+    download of that state."""
+    import torch
+    sc = scenes.dam_break(16, (40, 20, 20), stable=True)
+    a = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext())
+    b = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext())
+    b.upload(sc.pos, sc.vel)
+    b.step(3)
+    pos2, vel2 = b.download()
+    want = []
+    for pos, vel in ((sc.pos, sc.vel), (pos2, vel2)):
+        b.upload(pos, vel)
+        b.step(1)
+        want.append(b.download()[0])
+    ins = [(torch.from_numpy(np.ascontiguousarray(p, np.float32)).pin_memory(),
+            torch.from_numpy(np.ascontiguousarray(v, np.float32)).pin_memory()) for p, v in ((sc.pos, sc.vel), (pos2, vel2))]
+    outs = [torch.empty((sc.n, 3), dtype=torch.float32).pin_memory() for _ in range(4)]
+    stream = torch.cuda.Stream()
+    for k in range(4):
+        a.step_host(ins[k % 2][0], ins[k % 2][1], outs[k], 1, stream)
+    a.host_fence(stream)
+    stream.synchronize()
+    for k in range(4):
+        assert bits_equal(outs[k].numpy(), want[k % 2]), k
