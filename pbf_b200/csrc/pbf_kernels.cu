@@ -22,39 +22,54 @@ namespace pbf {
 // ---------------------------------------------------------------------------
 // a1 + a2: predict, bound, hash, histogram (one arrival ticket per particle)
 // ---------------------------------------------------------------------------
-template <bool PREDICT>
+template <bool PREDICT, int U>
 __global__ void __launch_bounds__(256, 8) k_hash(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
                                               int* __restrict__ cell, int* __restrict__ ticket, int* __restrict__ cnt,
                                               int* __restrict__ err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // Each warp takes U rounds of 32 consecutive slots; the loads, and then the
+    // histogram atomics, of all rounds are in flight together.
     const int lane = threadIdx.x & 31;
-    int key = -1;
-    if (i < p.n) {
-        const SceneView sc = scene_of(p, i);
-        f3 xi = make3(x[i]);
-        if (PREDICT) {
-            f3 vi = make3(v[i]);
-            predict(p, sc, xi, vi);
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int key[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const long long i = (w * U + u) * 32 + lane;
+        key[u] = -1;
+        if (i < p.n) {
+            const SceneView sc = scene_of(p, (int)i);
+            f3 xi = make3(x[i]);
+            if (PREDICT) {
+                f3 vi = make3(v[i]);
+                predict(p, sc, xi, vi);
+            }
+            if (!(isfinite(xi.x) && isfinite(xi.y) && isfinite(xi.z))) atomicOr(err, DEVERR_NONFINITE);
+            key[u] = cell_key(p, sc, xi);
         }
-        if (!(isfinite(xi.x) && isfinite(xi.y) && isfinite(xi.z))) atomicOr(err, DEVERR_NONFINITE);
-        key = cell_key(p, sc, xi);
     }
     // Run-aggregated histogram: slots are in cell order from the previous substep,
     // so equal keys come in runs; one atomic per run of equal keys in the warp.
     // (The ticket is only an arrival order; k_reorder makes the order stable.)
-    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
-    const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
-    const unsigned upto = starts & (0xffffffffu >> (31 - lane));  // run starts at or below this lane
-    const int leader = 31 - __clz(upto);
-    const unsigned above = starts & ~(0xffffffffu >> (31 - lane));
-    const int end = above ? __ffs(above) - 1 : 32;  // first run start above this lane
-    const int rank = lane - leader;
-    int base = 0;
-    if (key >= 0 && lane == leader) base = atomicAdd(&cnt[key], end - leader);
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (i < p.n) {
-        cell[i] = key;
-        ticket[i] = base + rank;
+    int base[U], leader[U], rank[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int prev = __shfl_up_sync(0xffffffffu, key[u], 1);
+        const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || prev != key[u]);
+        const unsigned upto = starts & (0xffffffffu >> (31 - lane));  // run starts at or below this lane
+        leader[u] = 31 - __clz(upto);
+        const unsigned above = starts & ~(0xffffffffu >> (31 - lane));
+        const int end = above ? __ffs(above) - 1 : 32;  // first run start above this lane
+        rank[u] = lane - leader[u];
+        base[u] = 0;
+        if (key[u] >= 0 && lane == leader[u]) base[u] = atomicAdd(&cnt[key[u]], end - leader[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int b = __shfl_sync(0xffffffffu, base[u], leader[u]);
+        const long long i = (w * U + u) * 32 + lane;
+        if (i < p.n) {
+            cell[i] = key[u];
+            ticket[i] = b + rank[u];
+        }
     }
 }
 
@@ -244,17 +259,31 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
 // a5: scatter by ticket (unordered within a cell), then a stable rank within the
 // cell and the reorder of the particle state into slot order (a6).
 // ---------------------------------------------------------------------------
+// Each thread takes U slots 256 apart within its block's tile of 256 U (the
+// loads of all U in flight together).
+template <int U>
 __global__ void __launch_bounds__(256) k_scatter(int n, const int* __restrict__ cell, const int* __restrict__ ticket,
                                                  const int* __restrict__ cell_start, int* __restrict__ tmp,
                                                  int* __restrict__ err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int dst = cell_start[cell[i]] + ticket[i];
-    if (dst < 0 || dst >= n) {  // counts and tickets disagree: report, never write out of bounds
-        atomicOr(err, DEVERR_BAD_INDEX);
-        return;
+    const long long i0 = (long long)blockIdx.x * blockDim.x * U + threadIdx.x;
+    int c[U], t[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const long long i = i0 + (long long)u * blockDim.x;
+        c[u] = i < n ? cell[i] : 0;
+        t[u] = i < n ? ticket[i] : 0;
     }
-    tmp[dst] = i;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const long long i = i0 + (long long)u * blockDim.x;
+        if (i >= n) break;
+        const int dst = cell_start[c[u]] + t[u];
+        if (dst < 0 || dst >= n) {  // counts and tickets disagree: report, never write out of bounds
+            atomicOr(err, DEVERR_BAD_INDEX);
+            continue;
+        }
+        tmp[dst] = (int)i;
+    }
 }
 
 template <bool PREDICT>
@@ -539,9 +568,10 @@ static inline int blocks_for(int n, int bs) { return (n + bs - 1) / bs; }
 static inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 void launch_hash(const KParams& p, bool predict_on, const float4* x, const float4* v, int* cell, int* ticket, int* cnt,
                  int* err, cudaStream_t st) {
-    const int b = blocks_for(p.n, 256);
-    if (predict_on) k_hash<true><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
-    else k_hash<false><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
+    constexpr int U = 4;
+    const int b = blocks_for(p.n, 256 * U);
+    if (predict_on) k_hash<true, U><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
+    else k_hash<false, U><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
 }
 
 size_t scan_status_bytes(int m) {
@@ -571,7 +601,8 @@ void launch_scan_const(const int* in, int* out, int m, void* status_ws, int* err
 
 void launch_scatter(int n, const int* cell, const int* ticket, const int* cell_start, int* tmp, int* err,
                     cudaStream_t st) {
-    k_scatter<<<blocks_for(n, 256), 256, 0, st>>>(n, cell, ticket, cell_start, tmp, err);
+    constexpr int U = 4;
+    k_scatter<U><<<blocks_for(n, 256 * U), 256, 0, st>>>(n, cell, ticket, cell_start, tmp, err);
 }
 
 void launch_reorder(const KParams& p, bool predict_on, const float4* x, const float4* v, const int* perm,
