@@ -191,6 +191,20 @@ int pbf_step(pbf_solver* s, int substeps, void* stream);
 int pbf_step_host(pbf_solver* s, const float* pos, const float* vel, float* pos_out, int substeps, void* stream);
 int pbf_host_fence(pbf_solver* s, void* stream);
 
+/* Changes the particle count of a single-scene solver to n (1 <= n <= the
+ * nParticles it was created with); the next pbf_step captures its graph again
+ * and needs a new upload first. Synchronises the device. */
+int pbf_resize(pbf_solver* s, int n);
+
+/* The state after the last pbf_step in slot order (cell order): AoS positions
+ * and velocities, each slot's index in the uploaded order, the key of the cell
+ * the slot was sorted into and the slot's rank within that cell. The next
+ * substep sorts stably by (key, rank), which is what a caller that splits and
+ * merges states (slab decomposition) needs to keep the order. Any pointer may
+ * be NULL; stream-ordered. */
+int pbf_download_sorted_device(pbf_solver* s, float* d_pos, float* d_vel, int* d_ids, int* d_key, int* d_rank,
+                               void* stream);
+
 /* Host copies of positions / velocities in original order (either may be NULL). */
 int pbf_download(pbf_solver* s, float* pos, float* vel);
 

@@ -116,6 +116,8 @@ _PROTOS = [
     ("pbf_download_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pbf_step_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     ("pbf_host_fence", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pbf_resize", C.c_int, [C.c_void_p, C.c_int]),
+    ("pbf_download_sorted_device", C.c_int, [C.c_void_p] + [C.c_void_p] * 5 + [C.c_void_p]),
     ("pbf_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("pbf_fetch", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     ("pbf_field_bytes", C.c_size_t, [C.c_void_p, C.c_int]),

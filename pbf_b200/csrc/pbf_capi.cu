@@ -94,6 +94,7 @@ struct pbf_solver {
     float grid_space[6]{}, boundary[6]{};
     KParams kp{};
     int n = 0, ncells = 0, nkeys = 0, stride = 0;  // ncells: real cells of scene 0
+    int capacity = 0;                              // particles the buffers hold (n <= capacity)
     std::vector<SceneView> scenes_h;
     SceneView* scenes_d = nullptr;  // scene table (batches)
     int* sid = nullptr;             // per slot: scene index (batches)
@@ -632,6 +633,7 @@ int create_common(const pbf_solver_parameter* para, int nscenes, const pbf_scene
     }
     s->nkeys = (int)keys;
     s->ncells = s->scenes_h[0].ncells;
+    s->capacity = s->n;
     s->stride = (s->n + 31) & ~31;
     const size_t n = s->n;
     const bool dbg = ext->debug != 0;
@@ -780,7 +782,7 @@ int pbf_step_host(pbf_solver* s, const float* pos, const float* vel, float* pos_
         HostPipe* hp = new (std::nothrow) HostPipe();
         if (!hp) return fail(PBF_ERR_ALLOC, "host allocation failed");
         s->hp = hp;
-        const size_t n = s->n;
+        const size_t n = s->capacity;
         cudaError_t e = cudaStreamCreateWithFlags(&hp->h2d, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&hp->d2h, cudaStreamNonBlocking);
         for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
@@ -824,6 +826,35 @@ int pbf_host_fence(pbf_solver* s, void* stream) {
     // copies of one direction complete in call order; the last copy-out comes
     // after its call's copy-in
     CK(cudaStreamWaitEvent((cudaStream_t)stream, s->hp->out_free[(s->hp->calls - 1) & 1], 0));
+    return PBF_OK;
+}
+
+int pbf_resize(pbf_solver* s, int n) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (s->scenes_h.size() != 1) return fail(PBF_ERR_INVALID, "pbf_resize needs a single-scene solver");
+    if (n < 1 || n > s->capacity) return fail(PBF_ERR_INVALID, "n (%d) outside [1, %d]", n, s->capacity);
+    CK(cudaDeviceSynchronize());  // nothing of the old size may still run
+    s->n = n;
+    s->para.nParticles = n;
+    s->scenes_h[0].pcount = n;
+    s->kp = make_kparams(*s);
+    if (s->exec) {  // grid sizes change: capture again at the next pbf_step
+        cudaGraphExecDestroy(s->exec);
+        s->exec = nullptr;
+    }
+    s->uploaded = false;
+    return PBF_OK;
+}
+
+int pbf_download_sorted_device(pbf_solver* s, float* d_pos, float* d_vel, int* d_ids, int* d_key, int* d_rank,
+                               void* stream) {
+    if (!s) return fail(PBF_ERR_INVALID, "null handle");
+    if (s->substeps == 0) return fail(PBF_ERR_STATE, "no substep has run since the upload");
+    cudaStream_t st = (cudaStream_t)stream;
+    launch_sorted_state(s->n, s->Sx, s->Sv, s->Sperm, s->cell_sorted, s->cell_start, d_pos, d_vel, d_ids, d_key,
+                        d_rank, st);
+    CK(cudaGetLastError());
+    s->last_stream = st;
     return PBF_OK;
 }
 

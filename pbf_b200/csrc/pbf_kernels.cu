@@ -540,6 +540,33 @@ __global__ void k_from_aos(int n, const float* __restrict__ pos, const float* __
     perm[i] = i;
 }
 
+// The state in slot order: AoS x and v, the loaded index of each slot, the key
+// of the cell the slot was sorted into and its rank within that cell (any
+// output may be null).
+__global__ void k_sorted_state(int n, const float4* __restrict__ x, const float4* __restrict__ v,
+                               const int* __restrict__ perm, const int* __restrict__ cell_sorted,
+                               const int* __restrict__ cell_start, float* __restrict__ pos, float* __restrict__ vel,
+                               int* __restrict__ ids, int* __restrict__ key, int* __restrict__ rank) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (pos) {
+        const float4 q = x[k];
+        pos[3 * k] = q.x;
+        pos[3 * k + 1] = q.y;
+        pos[3 * k + 2] = q.z;
+    }
+    if (vel) {
+        const float4 q = v[k];
+        vel[3 * k] = q.x;
+        vel[3 * k + 1] = q.y;
+        vel[3 * k + 2] = q.z;
+    }
+    if (ids) ids[k] = perm[k];
+    const int c = cell_sorted[k];
+    if (key) key[k] = c;
+    if (rank) rank[k] = k - cell_start[c];
+}
+
 // slot order -> original order, AoS xyz
 __global__ void k_to_aos(int n, const float4* __restrict__ a, const int* __restrict__ perm, float* __restrict__ out,
                          int* __restrict__ err) {
@@ -657,6 +684,13 @@ void launch_from_aos(int n, const float* pos, const float* vel, float4* x, float
 
 void launch_to_aos(int n, const float4* a, const int* perm, float* out, int* err, cudaStream_t st) {
     k_to_aos<<<blocks_for(n, 256), 256, 0, st>>>(n, a, perm, out, err);
+}
+
+void launch_sorted_state(int n, const float4* x, const float4* v, const int* perm, const int* cell_sorted,
+                         const int* cell_start, float* pos, float* vel, int* ids, int* key, int* rank,
+                         cudaStream_t st) {
+    k_sorted_state<<<blocks_for(n, 256), 256, 0, st>>>(n, x, v, perm, cell_sorted, cell_start, pos, vel, ids, key,
+                                                       rank);
 }
 
 void launch_copy4(int n, const float4* a, float4* b, cudaStream_t st) {

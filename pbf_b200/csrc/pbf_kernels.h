@@ -50,6 +50,9 @@ void launch_from_aos(int n, const float* pos, const float* vel, float4* x, float
                      cudaStream_t st);
 void launch_to_aos(int n, const float4* a, const int* perm, float* out, int* err, cudaStream_t st);
 void launch_copy4(int n, const float4* a, float4* b, cudaStream_t st);
+void launch_sorted_state(int n, const float4* x, const float4* v, const int* perm, const int* cell_sorted,
+                         const int* cell_start, float* pos, float* vel, int* ids, int* key, int* rank,
+                         cudaStream_t st);
 
 // Records the message returned by pbf_last_error() for this thread; returns code.
 int set_last_error(int code, const char* msg);

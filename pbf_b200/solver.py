@@ -152,6 +152,20 @@ class Solver:
         """Makes `stream` wait for every copy issued by step_host so far."""
         check(lib().pbf_host_fence(self._h, _stream_handle(stream)))
 
+    def resize(self, n: int) -> None:
+        """Particle count of a single-scene solver (<= the count it was created
+        with); needs a new upload before the next step."""
+        check(lib().pbf_resize(self._h, int(n)))
+        self.n = int(n)
+
+    def download_sorted_device(self, pos=None, vel=None, ids=None, key=None, rank=None, stream=None) -> None:
+        """The state after the last step in slot order into device tensors: n x 3
+        float32 pos / vel, int32 ids (index in the uploaded order), key (cell the
+        slot was sorted into) and rank (slot within that cell); any may be None."""
+        ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        check(lib().pbf_download_sorted_device(self._h, ptr(pos), ptr(vel), ptr(ids), ptr(key), ptr(rank),
+                                               _stream_handle(stream)))
+
     def stats(self, raise_on_error: bool = True) -> dict:
         st = Stats()
         rc = lib().pbf_get_stats(self._h, C.byref(st))
