@@ -595,10 +595,17 @@ static inline int blocks_for(int n, int bs) { return (n + bs - 1) / bs; }
 static inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 void launch_hash(const KParams& p, bool predict_on, const float4* x, const float4* v, int* cell, int* ticket, int* cnt,
                  int* err, cudaStream_t st) {
-    constexpr int U = 4;
-    const int b = blocks_for(p.n, 256 * U);
-    if (predict_on) k_hash<true, U><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
-    else k_hash<false, U><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
+    // four rounds per warp once there are enough particles to fill the device
+    // with them (about 1 M); below that, one round keeps more blocks resident
+    if (p.n >= (1 << 20)) {
+        const int b = blocks_for(p.n, 256 * 4);
+        if (predict_on) k_hash<true, 4><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
+        else k_hash<false, 4><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
+    } else {
+        const int b = blocks_for(p.n, 256);
+        if (predict_on) k_hash<true, 1><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
+        else k_hash<false, 1><<<b, 256, 0, st>>>(p, x, v, cell, ticket, cnt, err);
+    }
 }
 
 size_t scan_status_bytes(int m) {
@@ -628,8 +635,8 @@ void launch_scan_const(const int* in, int* out, int m, void* status_ws, int* err
 
 void launch_scatter(int n, const int* cell, const int* ticket, const int* cell_start, int* tmp, int* err,
                     cudaStream_t st) {
-    constexpr int U = 4;
-    k_scatter<U><<<blocks_for(n, 256 * U), 256, 0, st>>>(n, cell, ticket, cell_start, tmp, err);
+    if (n >= (1 << 20)) k_scatter<4><<<blocks_for(n, 256 * 4), 256, 0, st>>>(n, cell, ticket, cell_start, tmp, err);
+    else k_scatter<1><<<blocks_for(n, 256), 256, 0, st>>>(n, cell, ticket, cell_start, tmp, err);
 }
 
 void launch_reorder(const KParams& p, bool predict_on, const float4* x, const float4* v, const int* perm,
