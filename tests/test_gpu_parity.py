@@ -189,7 +189,8 @@ def test_grid_build_vs_reference_cpu_buildNeiborhood():
         assert got == want, k
 
 
-@pytest.mark.parametrize("m", [1, 31, 4095, 4096, 4097, 64 ** 3, 1_000_003, 8_192_001])
+@pytest.mark.parametrize("m", [1, 31, 2047, 2049, 4095, 4096, 4097, 64 ** 3, 1_000_003, (1 << 22) - 1, 1 << 22,
+                               8_192_001])
 def test_scan_matches_exclusive_prefix(m):
     """pbf_scan_exclusive_i32 on the shape of test/testPrefixSum.cpp:65-85
     (values rand()%16) and on ragged / large sizes; the total lands at out[m]."""
@@ -207,7 +208,7 @@ def test_scan_matches_exclusive_prefix(m):
     assert np.array_equal(d_in.cpu().numpy(), a), "input must be left unchanged"
 
 
-@pytest.mark.parametrize("m", [1, 4099, 262144 + 3])
+@pytest.mark.parametrize("m", [1, 4099, 262144 + 3, (1 << 22) + 3])
 @pytest.mark.parametrize("shift", [1, 3])
 def test_scan_unaligned_pointers(m, shift):
     """Arrays that do not start on a 16-byte boundary take the scalar path of the
