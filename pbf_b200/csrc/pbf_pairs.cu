@@ -84,7 +84,7 @@ template <int V> using vec_t = typename std::conditional<V == 1, float, float2>:
 
 // r = x_k - x_j, |r|^2 = fma(z, z, fma(y, y, x*x)), Wpoly6 (when NEED_W) and the
 // spiky gradient of V pairs, exactly as w_poly6 / grad_spiky (pbf_device.cuh)
-// evaluate one pair; components outside `valid` give w = +0 and g = +0.
+// evaluate one pair; components outside `valid` give w = +0 and g = +0 or -0.
 template <typename T, bool NEED_W>
 __device__ __forceinline__ void pair_terms(const KParams& p, const f3& xk, const T3<T>& xj, unsigned valid, T3<T>& r,
                                            T& w, T3<T>& g) {
@@ -99,7 +99,10 @@ __device__ __forceinline__ void pair_terms(const KParams& p, const f3& xk, const
     const T d = vfma(vneg(r2), y, bc<T>(p.h));  // h - |r|
     const T s = vmul(vmul(vmul(bc<T>(p.spiky_c), d), d), y);
     const unsigned keep = valid & ~(gt_mask(rl, p.h) | lt_mask(rl, p.rmin));
-    g = {keep_only(vmul(s, r.x), keep), keep_only(vmul(s, r.y), keep), keep_only(vmul(s, r.z), keep)};
+    // the mask on the magnitude: a dropped pair gives a gradient of +0 or -0,
+    // which leaves every sum it enters unchanged (no accumulator is ever -0)
+    const T sk = keep_only(s, keep);
+    g = {vmul(sk, r.x), vmul(sk, r.y), vmul(sk, r.z)};
 }
 
 // The dp pair weight (lambda_i + lambda_j) + s_corr (cu:193-195, Scorr cuh:142-144)
