@@ -229,7 +229,8 @@ int pbf_build_grid(pbf_solver* s, void* stream);
 int pbf_get_layout(const pbf_solver* s, int* ncells, int* stride, int* max_neighbors);
 
 /* Profiling (ext.profile = 1): milliseconds per stage in the last substep, summed
- * over the launches of each stage. Stages: 0 hash, 1 scan, 2 scatter,
+ * over the launches of each stage. Stages: 0 hash (0 within a substep: the
+ * previous substep's vorticity pass hashes the state it writes), 1 scan, 2 scatter,
  * 3 reorder, 4 neighbours, 5 lambda, 6 dp, 7 velocity, 8 curl, 9 vorticity,
  * 10 copy, 11 density measurement, 12 warm-start MLP. */
 #define PBF_NUM_STAGES 13

@@ -373,7 +373,9 @@ int enqueue_substep(pbf_solver* s, cudaStream_t st) {
     int* err = &s->dstats->err;
     DevStats* ds = s->dstats;
     Prof P{s, st, s->ext.profile != 0};
-    P(ST_HASH, [&] { launch_hash(kp, true, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st); });
+    // (the grid hash of this substep's predicted positions -- cell keys, tickets
+    // and counts -- was done by the previous substep's vorticity pass, or by the
+    // upload or grid build that set the state)
     if (dbg) cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
     P(ST_SCAN, [&] { launch_scan(s->cnt, s->cell_start, s->nkeys, s->scan_ws, err, st); });
     P(ST_SCATTER, [&] { launch_scatter(n, s->cell, s->ticket, s->cell_start, s->tmp, err, st); });
@@ -459,7 +461,7 @@ int enqueue_substep(pbf_solver* s, cudaStream_t st) {
     P(ST_CURL, [&] { launch_curl(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->omega, s->vw, st); });
     P(ST_VORT, [&] {
         launch_vort(kp, dbg, s->Px, s->vw, s->omega, s->nbr, s->ncnt, s->Sx, s->Sv, s->Pperm, s->Sperm,
-                    s->vort_dbg, s->visc_dbg, st);
+                    s->vort_dbg, s->visc_dbg, s->cell, s->ticket, s->cnt, err, st);
     });
     return PBF_OK;
 }
@@ -729,6 +731,11 @@ int pbf_upload_device(pbf_solver* s, const float* d_pos, const float* d_vel, int
     launch_from_aos(n, d_pos, d_vel, s->Sx, s->Sv, s->Sperm, &s->dstats->err, st);
     CK(cudaGetLastError());
     CK(cudaMemsetAsync(s->lam_acc, 0, sizeof(float) * n, st));
+    // the first substep's grid hash (later substeps get theirs from the
+    // vorticity pass before them)
+    CK(cudaMemsetAsync(s->cnt, 0, sizeof(int) * (size_t)s->nkeys, st));
+    launch_hash(s->kp, true, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, &s->dstats->err, st);
+    CK(cudaGetLastError());
     s->last_stream = st;
     s->uploaded = true;
     s->substeps = s->total_iters = s->fallbacks = 0;
@@ -864,6 +871,7 @@ int pbf_build_grid(pbf_solver* s, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const KParams& kp = s->kp;
     int* err = &s->dstats->err;
+    CK(cudaMemsetAsync(s->cnt, 0, sizeof(int) * (size_t)s->nkeys, st));  // drop the next substep's counts
     launch_hash(kp, false, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st);
     if (s->hash_dbg) CK(cudaMemcpyAsync(s->hash_dbg, s->cell, sizeof(int) * s->n, cudaMemcpyDeviceToDevice, st));
     launch_scan(s->cnt, s->cell_start, s->nkeys, s->scan_ws, err, st);
@@ -876,6 +884,9 @@ int pbf_build_grid(pbf_solver* s, void* stream) {
     CK(cudaMemcpyAsync(s->Sx, s->Px, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s->Sv, s->Pv, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s->Sperm, s->Pperm, sizeof(int) * s->n, cudaMemcpyDeviceToDevice, st));
+    // the next substep's grid hash of that state (the scan left the counts zero)
+    launch_hash(kp, true, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, err, st);
+    CK(cudaGetLastError());
     s->last_stream = st;
     return PBF_OK;
 }

@@ -271,6 +271,23 @@ __device__ __forceinline__ void predict(const KParams& p, const SceneView& sc, f
     bound_particle(p, sc, x);
 }
 
+// Run-aggregated histogram of one warp's cell keys (every lane of the warp
+// calls it; key < 0: no particle). Slots are in cell order from the previous
+// substep, so equal keys come in runs: one atomic per run. Returns the lane's
+// ticket, an arrival order within its cell (the reorder makes the order stable).
+__device__ __forceinline__ int warp_histogram(int key, int* cnt) {
+    const int lane = threadIdx.x & 31;
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const unsigned starts = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+    const unsigned upto = starts & (0xffffffffu >> (31 - lane));  // run starts at or below this lane
+    const int leader = 31 - __clz(upto);
+    const unsigned above = starts & ~(0xffffffffu >> (31 - lane));
+    const int end = above ? __ffs(above) - 1 : 32;  // first run start above this lane
+    int base = 0;
+    if (key >= 0 && lane == leader) base = atomicAdd(&cnt[key], end - leader);
+    return __shfl_sync(0xffffffffu, base, leader) + (lane - leader);
+}
+
 // computeDimID (cuh:156-160): truncation toward zero
 __device__ __forceinline__ void cell_dims(const KParams& p, const SceneView& sc, const f3& x, int d[3]) {
     d[0] = (int)((x.x - sc.gmin[0]) * p.inv_cell);

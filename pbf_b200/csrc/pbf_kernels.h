@@ -39,11 +39,13 @@ void launch_velocity(const KParams& p, const float4* x, const float4* xold, floa
 // Curl: omega = (w, |w|) and vw = (v, |w|) per particle.
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
                  float4* vw, cudaStream_t st);
-// Vorticity + XSPH from vw = (v, |w|) and omega; also writes the final state:
-// xout = x, vout = v + dv, perm_out = perm_in.
+// Vorticity + XSPH from vw = (v, |w|) and omega; also writes the final state
+// (xout = x, vout = v + dv, perm_out = perm_in) and the next substep's grid hash
+// of that state: cell key and ticket per slot, counts added to hist (which the
+// scan left zero).
 void launch_vort(const KParams& p, bool debug, const float4* x, const float4* vw, const float4* omega, const int* nbr,
                  const int* ncnt, float4* xout, float4* vout, const int* perm_in, int* perm_out, float4* vort,
-                 float4* visc, cudaStream_t st);
+                 float4* visc, int* cell, int* ticket, int* hist, int* err, cudaStream_t st);
 void launch_density_error(const KParams& p, const float4* x, const int* nbr, const int* ncnt,
                           unsigned long long* max_bits, double* sum, const int* skip, cudaStream_t st);
 void launch_from_aos(int n, const float* pos, const float* vel, float4* x, float4* v, int* perm, int* err,

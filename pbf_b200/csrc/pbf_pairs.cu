@@ -521,20 +521,23 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
 // ---------------------------------------------------------------------------
 // a13: vorticity confinement and XSPH, applied to v
 // (calculateVorticityAndViscosity cu:217-239, applyVorticityAndViscosity cu:24-29);
-// also writes the substep's final state (x, v, perm) for the next substep
+// also writes the substep's final state (x, v, perm) for the next substep, and
+// with the final x and v in registers does the next substep's grid hash (a1 +
+// a2: prediction, wall clamp, cell key and its histogram), which therefore needs
+// no pass of its own.
 // ---------------------------------------------------------------------------
+// One particle (team tm); returns its next cell key on the team's first thread
+// and -1 on the others.
 template <bool DEBUG, int L, int V>
-__global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restrict__ x, const float4* __restrict__ vw,
-                                              const float4* __restrict__ omega, const int* __restrict__ nbr,
-                                              const int* __restrict__ ncnt, float4* __restrict__ xout,
-                                              float4* __restrict__ vout, const int* __restrict__ perm_in,
-                                              int* __restrict__ perm_out, float4* __restrict__ vort_out,
-                                              float4* __restrict__ visc_out) {
+__device__ __forceinline__ int vort_one(const KParams& p, const Team<L>& tm, int k, const float4* __restrict__ x,
+                                        const float4* __restrict__ vw, const float4* __restrict__ omega,
+                                        const int* __restrict__ nbr, const int* __restrict__ ncnt,
+                                        float4* __restrict__ xout, float4* __restrict__ vout,
+                                        const int* __restrict__ perm_in, int* __restrict__ perm_out,
+                                        float4* __restrict__ vort_out, float4* __restrict__ visc_out,
+                                        int* __restrict__ err) {
     using T = vec_t<V>;
     constexpr int P = L * V, B = batches<V>();  // two 16-byte gathers per entry
-    const Team<L> tm = team_of<L>();
-    const int k = tm.k;
-    if (k >= p.n) return;  // uniform over the team
     const f3 xk = make3(x[k]);
     const f3 vk = make3(vw[k]);
     const int cnt = ncnt[k];
@@ -568,19 +571,49 @@ __global__ void __launch_bounds__(256) k_vort(KParams p, const float4* __restric
     }
     const f3 pvs = team_sum3<L>(fold3(pv), tm.mask);
     f3 etas = team_sum3<L>(fold3(eta), tm.mask);
-    if (tm.t != 0) return;
+    if (tm.t != 0) return -1;
     const float el = __fsqrt_rn(dot_fma(etas, etas));
     if ((double)el > 1e-3) etas = {__fdiv_rn(etas.x, el), __fdiv_rn(etas.y, el), __fdiv_rn(etas.z, el)};
     const f3 cr = cross3(etas, make3(omega[k]));
     const f3 fv = {p.vort_eps * cr.x, p.vort_eps * cr.y, p.vort_eps * cr.z};
     const f3 vs = {p.visc_c * pvs.x, p.visc_c * pvs.y, p.visc_c * pvs.z};
     const f3 t = {p.dt * fv.x + vs.x, p.dt * fv.y + vs.y, p.dt * fv.z + vs.z};
+    f3 vn = {vk.x + t.x, vk.y + t.y, vk.z + t.z};
     xout[k] = make_float4(xk.x, xk.y, xk.z, 0.0f);
-    vout[k] = make_float4(vk.x + t.x, vk.y + t.y, vk.z + t.z, 0.0f);
+    vout[k] = make_float4(vn.x, vn.y, vn.z, 0.0f);
     perm_out[k] = perm_in[k];
     if (DEBUG) {
         vort_out[k] = make_float4(fv.x, fv.y, fv.z, 0.0f);
         visc_out[k] = make_float4(vs.x, vs.y, vs.z, 0.0f);
+    }
+    // the next substep's prediction and cell key (as k_hash computes them from
+    // the state just written)
+    const SceneView sc = scene_of(p, k);
+    f3 xq = xk;
+    predict(p, sc, xq, vn);
+    if (!(isfinite(xq.x) && isfinite(xq.y) && isfinite(xq.z))) atomicOr(err, DEVERR_NONFINITE);
+    return cell_key(p, sc, xq);
+}
+
+template <bool DEBUG, int L, int V>
+__global__ void __launch_bounds__(256, 4) k_vort(KParams p, const float4* __restrict__ x, const float4* __restrict__ vw,
+                                              const float4* __restrict__ omega, const int* __restrict__ nbr,
+                                              const int* __restrict__ ncnt, float4* __restrict__ xout,
+                                              float4* __restrict__ vout, const int* __restrict__ perm_in,
+                                              int* __restrict__ perm_out, float4* __restrict__ vort_out,
+                                              float4* __restrict__ visc_out, int* __restrict__ cell,
+                                              int* __restrict__ ticket, int* __restrict__ hist, int* __restrict__ err) {
+    const Team<L> tm = team_of<L>();
+    const int k = tm.k;
+    int key = -1;
+    if (k < p.n)  // uniform over the team
+        key = vort_one<DEBUG, L, V>(p, tm, k, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort_out,
+                                    visc_out, err);
+    // the next substep's histogram (every lane of the warp takes part)
+    const int tk = warp_histogram(key, hist);
+    if (key >= 0) {
+        cell[k] = key;
+        ticket[k] = tk;
     }
 }
 
@@ -642,16 +675,16 @@ void launch_curl(const KParams& p, const float4* x, const float4* v, const int* 
 
 void launch_vort(const KParams& p, bool debug, const float4* x, const float4* vw, const float4* omega, const int* nbr,
                  const int* ncnt, float4* xout, float4* vout, const int* perm_in, int* perm_out, float4* vort,
-                 float4* visc, cudaStream_t st) {
+                 float4* visc, int* cell, int* ticket, int* hist, int* err, cudaStream_t st) {
     with_lanes(p.lanes, [&](auto c) {
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
         const int b = team_blocks(p.n, L, p.block);
         if (debug)
             k_vort<true, L, V><<<b, p.block, 0, st>>>(p, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort,
-                                                      visc);
+                                                      visc, cell, ticket, hist, err);
         else
             k_vort<false, L, V><<<b, p.block, 0, st>>>(p, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out,
-                                                       vort, visc);
+                                                       vort, visc, cell, ticket, hist, err);
     });
 }
 
