@@ -150,8 +150,8 @@ def run_reference(args) -> int:
     from pbf_b200 import scenes
     sc = scenes.dam_break(32, (80, 40, 40), stable=False)
     line = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "impl": "reference", "dtype": "f32", "data": "synthetic",
-            "config": workload_config(args)}
+            "higher_is_better": True, "impl": "reference", "scaling": "weak", "dtype": "f32",
+            "data": "synthetic", "config": workload_config(args)}
     if not O.refcpu_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver not built (oracle/_ref missing)"}))
         return 0
