@@ -43,15 +43,22 @@ __device__ __forceinline__ float2 keep_only(float2 a, unsigned keep) {
 __device__ __forceinline__ float fold(float a) { return a; }
 __device__ __forceinline__ float fold(float2 a) { return a.x + a.y; }
 
-// pbf_rsqrt (pbf_device.cuh) on each component
-__device__ __forceinline__ float vrsqrt(float x) { return pbf_rsqrt(x); }
-__device__ __forceinline__ float2 vrsqrt(float2 x) {
-    const float2 hx = vmul(bc<float2>(0.5f), x);
-    float2 y = make_float2(__int_as_float(0x5f3759df - (__float_as_int(x.x) >> 1)),
-                           __int_as_float(0x5f3759df - (__float_as_int(x.y) >> 1)));
+// Negated pbf_rsqrt (pbf_device.cuh) on each component, without a negation:
+// the steps y <- y fma(-x/2, y^2, 3/2) take -x/2 as the product (-0.5) x, and the
+// last step multiplies by fma(x/2, y^2, -3/2) = -fma(-x/2, y^2, 3/2) (round to
+// nearest is symmetric in sign), which yields exactly -pbf_rsqrt(x).
+__device__ __forceinline__ unsigned rsqrt_seed(float x) { return 0x5f3759df - (__float_as_int(x) >> 1); }
+__device__ __forceinline__ float rsqrt_seed_v(float x) { return __int_as_float(rsqrt_seed(x)); }
+__device__ __forceinline__ float2 rsqrt_seed_v(float2 x) {
+    return make_float2(__int_as_float(rsqrt_seed(x.x)), __int_as_float(rsqrt_seed(x.y)));
+}
+template <typename T> __device__ __forceinline__ T vrsqrt_neg(T x) {
+    const T hx = vmul(bc<T>(0.5f), x);
+    const T nhx = vmul(bc<T>(-0.5f), x);
+    T y = rsqrt_seed_v(x);
 #pragma unroll
-    for (int i = 0; i < 3; ++i) y = vmul(y, vfma(vneg(hx), vmul(y, y), bc<float2>(1.5f)));
-    return y;
+    for (int i = 0; i < 2; ++i) y = vmul(y, vfma(nhx, vmul(y, y), bc<T>(1.5f)));
+    return vmul(y, vfma(hx, vmul(y, y), bc<T>(-1.5f)));
 }
 
 template <typename T> struct T3 {
@@ -67,9 +74,11 @@ __device__ __forceinline__ f3 fold3(const T3<float2>& a) { return {fold(a.x), fo
 // (fma(a_y, b_z, -(a_z b_y)), fma(a_z, b_x, -(a_x b_z)), fma(a_x, b_y, -(a_y b_x))).
 // (A packed multiply whose only use is an add may be fused by the code generator,
 // so every product that meets an addition in these passes is an explicit fma.)
+// -(a b) is taken as (a b) (-1), which is the same value, signed zeros included.
 template <typename T> __device__ __forceinline__ T3<T> cross3v(const T3<T>& a, const T3<T>& b) {
-    return {vfma(a.y, b.z, vneg(vmul(a.z, b.y))), vfma(a.z, b.x, vneg(vmul(a.x, b.z))),
-            vfma(a.x, b.y, vneg(vmul(a.y, b.x)))};
+    const T m1 = bc<T>(-1.0f);
+    return {vfma(a.y, b.z, vmul(vmul(a.z, b.y), m1)), vfma(a.z, b.x, vmul(vmul(a.x, b.z), m1)),
+            vfma(a.x, b.y, vmul(vmul(a.y, b.x), m1))};
 }
 
 // xyz (or .w) of V gathered float4s as one packet
@@ -85,20 +94,25 @@ template <int V> using vec_t = typename std::conditional<V == 1, float, float2>:
 // r = x_k - x_j, |r|^2 = fma(z, z, fma(y, y, x*x)), Wpoly6 (when NEED_W) and the
 // spiky gradient of V pairs, exactly as w_poly6 / grad_spiky (pbf_device.cuh)
 // evaluate one pair; components outside `valid` give w = +0 and g = +0 or -0.
+// Every difference a - b is fma(b, -1, a), which rounds the same exact value
+// once (signed zeros included), and the rsqrt comes negated (ny = -y), so no
+// operand needs a negation of its own: h - |r| = fma(|r|^2, ny, h), |r| > h is
+// |r|^2 ny < -h, and ((c d) d) y = ((-c d) d) ny.
 template <typename T, bool NEED_W>
 __device__ __forceinline__ void pair_terms(const KParams& p, const f3& xk, const T3<T>& xj, unsigned valid, T3<T>& r,
                                            T& w, T3<T>& g) {
-    r = {vsub(bc<T>(xk.x), xj.x), vsub(bc<T>(xk.y), xj.y), vsub(bc<T>(xk.z), xj.z)};
+    const T m1 = bc<T>(-1.0f);
+    r = {vfma(xj.x, m1, bc<T>(xk.x)), vfma(xj.y, m1, bc<T>(xk.y)), vfma(xj.z, m1, bc<T>(xk.z))};
     const T r2 = vfma(r.z, r.z, vfma(r.y, r.y, vmul(r.x, r.x)));
     if (NEED_W) {
-        const T t = vsub(bc<T>(p.h2), r2);
+        const T t = vfma(r2, m1, bc<T>(p.h2));
         w = keep_only(vmul(bc<T>(p.poly6_c), vmul(vmul(t, t), t)), valid & ~gt_mask(r2, p.h2));
     }
-    const T y = vrsqrt(vmax(r2, 1e-30f));
-    const T rl = vmul(r2, y);                  // |r| for the cutoff
-    const T d = vfma(vneg(r2), y, bc<T>(p.h));  // h - |r|
-    const T s = vmul(vmul(vmul(bc<T>(p.spiky_c), d), d), y);
-    const unsigned keep = valid & ~(gt_mask(rl, p.h) | lt_mask(rl, p.rmin));
+    const T ny = vrsqrt_neg(vmax(r2, 1e-30f));
+    const T nrl = vmul(r2, ny);               // -|r| for the cutoff
+    const T d = vfma(r2, ny, bc<T>(p.h));      // h - |r|
+    const T s = vmul(vmul(vmul(bc<T>(-p.spiky_c), d), d), ny);
+    const unsigned keep = valid & ~(lt_mask(nrl, -p.h) | gt_mask(nrl, -p.rmin));
     // the mask on the magnitude: a dropped pair gives a gradient of +0 or -0,
     // which leaves every sum it enters unchanged (no accumulator is ever -0)
     const T sk = keep_only(s, keep);
@@ -114,7 +128,9 @@ __device__ __forceinline__ float2 vpow(float2 q, const KParams& p) {
 template <typename T> __device__ __forceinline__ T dp_weight(const KParams& p, float li, T lj, T w) {
     const T q = vmul(w, bc<T>(p.inv_wdq));
     T pw;
-    if (p.n_int > 0) {
+    if (p.n_int == 4) {  // the usual n = 4 without a loop: ((q q) q) q
+        pw = vmul(vmul(vmul(q, q), q), q);
+    } else if (p.n_int > 0) {
         pw = q;
         for (int i = 1; i < p.n_int; ++i) pw = vmul(pw, q);
     } else {
