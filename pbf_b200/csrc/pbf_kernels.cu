@@ -367,7 +367,11 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
         const float ey = dy == 0 ? 0.0f : fmaxf(gy - m, 0.0f);
         const float rem = hm2 - ez * ez - ey * ey;
         if (!(rem >= 0.0f)) return;
-        const float w = sqrtf(rem) + m;
+        // the half-width only bounds the candidates (the margin m of at least
+        // 1e-3 h is far above the approximate root's relative error of 2^-22)
+        float w;
+        asm("sqrt.approx.f32 %0, %1;" : "=f"(w) : "f"(rem));
+        w += m;
         const int xa = max(x0, (int)floorf((xk.x - w - sc.gmin[0]) * p.inv_cell));
         const int xb = min(x1, (int)floorf((xk.x + w - sc.gmin[0]) * p.inv_cell));
         if (xa > xb) return;
@@ -376,7 +380,8 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
         e = cell_start[row + xb + 1];
     };
     // candidates [s, e) in slot order, four positions in flight; |r|^2 of two
-    // candidates per packed instruction (the same IEEE operations as dot_fma)
+    // candidates per packed instruction (the same IEEE operations as dot_fma;
+    // x_k - x_j as fma(x_j, -1, x_k), the same single rounding of the difference)
     auto scan_row = [&](int s, int e) {
         for (int j0 = s; j0 < e && c < cap; j0 += 4) {
             float4 xj[4];
@@ -385,9 +390,10 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
             float r2[4];
 #pragma unroll
             for (int u = 0; u < 4; u += 2) {
-                const float2 rx = vsub(bc<float2>(xk.x), make_float2(xj[u].x, xj[u + 1].x));
-                const float2 ry = vsub(bc<float2>(xk.y), make_float2(xj[u].y, xj[u + 1].y));
-                const float2 rz = vsub(bc<float2>(xk.z), make_float2(xj[u].z, xj[u + 1].z));
+                const float2 m1 = bc<float2>(-1.0f);
+                const float2 rx = vfma(make_float2(xj[u].x, xj[u + 1].x), m1, bc<float2>(xk.x));
+                const float2 ry = vfma(make_float2(xj[u].y, xj[u + 1].y), m1, bc<float2>(xk.y));
+                const float2 rz = vfma(make_float2(xj[u].z, xj[u + 1].z), m1, bc<float2>(xk.z));
                 const float2 d2 = vfma(rz, rz, vfma(ry, ry, vmul(rx, rx)));
                 r2[u] = d2.x;
                 r2[u + 1] = d2.y;
