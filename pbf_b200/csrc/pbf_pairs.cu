@@ -97,7 +97,11 @@ template <int V> using vec_t = typename std::conditional<V == 1, float, float2>:
 // Every difference a - b is fma(b, -1, a), which rounds the same exact value
 // once (signed zeros included), and the rsqrt comes negated (ny = -y), so no
 // operand needs a negation of its own: h - |r| = fma(|r|^2, ny, h), |r| > h is
-// |r|^2 ny < -h, and ((c d) d) y = ((-c d) d) ny.
+// |r|^2 ny < -h, and ((c d) d) y = ((-c d) d) ny. The poly6 cutoff |r|^2 > h^2
+// is max(h^2 - |r|^2, +0) (the difference is negative exactly when the same
+// rounded |r|^2 exceeds h^2, and c (+0)^3 = +0). A padding entry is the particle
+// itself (r = +0, |r| below rmin), which the gradient's cutoff already drops;
+// only its density weight needs `valid`.
 template <typename T, bool NEED_W>
 __device__ __forceinline__ void pair_terms(const KParams& p, const f3& xk, const T3<T>& xj, unsigned valid, T3<T>& r,
                                            T& w, T3<T>& g) {
@@ -105,14 +109,14 @@ __device__ __forceinline__ void pair_terms(const KParams& p, const f3& xk, const
     r = {vfma(xj.x, m1, bc<T>(xk.x)), vfma(xj.y, m1, bc<T>(xk.y)), vfma(xj.z, m1, bc<T>(xk.z))};
     const T r2 = vfma(r.z, r.z, vfma(r.y, r.y, vmul(r.x, r.x)));
     if (NEED_W) {
-        const T t = vfma(r2, m1, bc<T>(p.h2));
-        w = keep_only(vmul(bc<T>(p.poly6_c), vmul(vmul(t, t), t)), valid & ~gt_mask(r2, p.h2));
+        const T t = vmax(vfma(r2, m1, bc<T>(p.h2)), 0.0f);
+        w = keep_only(vmul(bc<T>(p.poly6_c), vmul(vmul(t, t), t)), valid);
     }
     const T ny = vrsqrt_neg(vmax(r2, 1e-30f));
     const T nrl = vmul(r2, ny);               // -|r| for the cutoff
     const T d = vfma(r2, ny, bc<T>(p.h));      // h - |r|
     const T s = vmul(vmul(vmul(bc<T>(-p.spiky_c), d), d), ny);
-    const unsigned keep = valid & ~(lt_mask(nrl, -p.h) | gt_mask(nrl, -p.rmin));
+    const unsigned keep = ~(lt_mask(nrl, -p.h) | gt_mask(nrl, -p.rmin));
     // the mask on the magnitude: a dropped pair gives a gradient of +0 or -0,
     // which leaves every sum it enters unchanged (no accumulator is ever -0)
     const T sk = keep_only(s, keep);
@@ -182,9 +186,9 @@ __device__ __forceinline__ void load_idx(const KParams& p, const int* __restrict
         }
 }
 
-// bit v: entry q + v exists
+// bit v: entry q + v exists (the callers have q < cnt, so bit 0 is always set)
 template <int V> __device__ __forceinline__ unsigned valid_bits(int q, int cnt) {
-    return V == 1 ? 1u : ((q < cnt ? 1u : 0u) | (q + 1 < cnt ? 2u : 0u));
+    return V == 1 ? 1u : (q + 1 < cnt ? 3u : 1u);
 }
 
 // Block-wide max and sum of a per-thread error, folded into one slot with a
