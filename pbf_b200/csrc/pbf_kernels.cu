@@ -336,8 +336,10 @@ __global__ void __launch_bounds__(256, 8) k_reorder(KParams p, const float4* __r
 // ---------------------------------------------------------------------------
 // Stencil radius RR as a constant (1: cells of h, 2: cells of h/2; 0: any radius,
 // read from p.radius). For RR > 0 the row ranges of a plane of cells are loaded
-// together and candidates are fetched four at a time, so a thread waits on a few
-// independent loads at once instead of one chain per row and per candidate.
+// together and candidates are fetched two at a time (a clipped row of cells of
+// h/2 holds a few, and wider batches leave more of their slots empty), so a
+// thread waits on a few independent loads at once instead of one chain per row
+// and per candidate.
 template <int RR>
 __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __restrict__ x,
                                                    const int* __restrict__ cell_start, int* __restrict__ nbr,
@@ -355,17 +357,21 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
     const int cap = p.max_nbr;
     const float m = p.h * 1e-3f + 1e-6f * (fabsf(xk.x) + fabsf(xk.y) + fabsf(xk.z));
     const float hm2 = (p.h + m) * (p.h + m);
-    // slot range [s, e) of stencil row (dy, dz), clipped to the sphere; empty when
-    // the row is outside the grid or farther than h
-    auto row_range = [&](int dy, int z, float ez, int& s, int& e) {
-        s = 0;
-        e = 0;
+    // squared distance from the particle to the y slab of stencil row dy (less
+    // the margin), +inf for a row outside the grid
+    auto row_ey2 = [&](int dy) {
         const int y = d[1] + dy;
-        if (y < 0 || y >= ny) return;
+        if (y < 0 || y >= ny) return INFINITY;
         const float gy = dy > 0 ? (sc.gmin[1] + (float)y * p.cell) - xk.y
                                 : xk.y - (sc.gmin[1] + (float)(y + 1) * p.cell);
         const float ey = dy == 0 ? 0.0f : fmaxf(gy - m, 0.0f);
-        const float rem = hm2 - ez * ez - ey * ey;
+        return ey * ey;
+    };
+    // slot range [s, e) of the stencil row in cell row y of plane z, clipped to
+    // the sphere (rem = (h + m)^2 - ez^2 - ey^2); empty when farther than h
+    auto row_clip = [&](int y, int z, float rem, int& s, int& e) {
+        s = 0;
+        e = 0;
         if (!(rem >= 0.0f)) return;
         // the half-width only bounds the candidates (the margin m of at least
         // 1e-3 h is far above the approximate root's relative error of 2^-22)
@@ -379,17 +385,18 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
         s = cell_start[row + xa];
         e = cell_start[row + xb + 1];
     };
-    // candidates [s, e) in slot order, four positions in flight; |r|^2 of two
+    // candidates [s, e) in slot order, NB positions in flight; |r|^2 of two
     // candidates per packed instruction (the same IEEE operations as dot_fma;
     // x_k - x_j as fma(x_j, -1, x_k), the same single rounding of the difference)
+    constexpr int NB = 2;  // candidates per batch (even; rows of cells of h/2 hold a few)
     auto scan_row = [&](int s, int e) {
-        for (int j0 = s; j0 < e && c < cap; j0 += 4) {
-            float4 xj[4];
+        for (int j0 = s; j0 < e && c < cap; j0 += NB) {
+            float4 xj[NB];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) xj[u] = x[min(j0 + u, e - 1)];
-            float r2[4];
+            for (int u = 0; u < NB; ++u) xj[u] = x[min(j0 + u, e - 1)];
+            float r2[NB];
 #pragma unroll
-            for (int u = 0; u < 4; u += 2) {
+            for (int u = 0; u < NB; u += 2) {
                 const float2 m1 = bc<float2>(-1.0f);
                 const float2 rx = vfma(make_float2(xj[u].x, xj[u + 1].x), m1, bc<float2>(xk.x));
                 const float2 ry = vfma(make_float2(xj[u].y, xj[u + 1].y), m1, bc<float2>(xk.y));
@@ -399,7 +406,7 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
                 r2[u + 1] = d2.y;
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < NB; ++u) {
                 const int j = j0 + u;
                 if (j >= e || c >= cap) break;
                 if (j == k) continue;
@@ -411,6 +418,13 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
         }
     };
     if (x0 <= x1) {
+        // the rows' y distances are the same in every plane
+        constexpr int W = RR > 0 ? 2 * RR + 1 : 1;
+        float ey2[W];
+        if (RR > 0) {
+#pragma unroll
+            for (int i = 0; i < W; ++i) ey2[i] = row_ey2(i - RR);
+        }
         for (int dz = -R; dz <= R && c < cap; ++dz) {
             const int z = d[2] + dz;
             if (z < 0 || z >= nz) continue;
@@ -419,17 +433,17 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
                                     : xk.z - (sc.gmin[2] + (float)(z + 1) * p.cell);
             const float ez = dz == 0 ? 0.0f : fmaxf(gz - m, 0.0f);
             if (ez * ez > hm2) continue;
+            const float hz = hm2 - ez * ez;
             if (RR > 0) {
-                constexpr int W = 2 * RR + 1;
-                int s[W > 0 ? W : 1], e[W > 0 ? W : 1];
+                int s[W], e[W];
 #pragma unroll
-                for (int i = 0; i < W; ++i) row_range(i - RR, z, ez, s[i], e[i]);
+                for (int i = 0; i < W; ++i) row_clip(d[1] + i - RR, z, hz - ey2[i], s[i], e[i]);
 #pragma unroll
                 for (int i = 0; i < W; ++i) scan_row(s[i], e[i]);
             } else {
                 for (int dy = -R; dy <= R && c < cap; ++dy) {
                     int s, e;
-                    row_range(dy, z, ez, s, e);
+                    row_clip(d[1] + dy, z, hz - row_ey2(dy), s, e);
                     scan_row(s, e);
                 }
             }
