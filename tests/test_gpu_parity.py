@@ -189,8 +189,8 @@ def test_grid_build_vs_reference_cpu_buildNeiborhood():
         assert got == want, k
 
 
-@pytest.mark.parametrize("m", [1, 31, 2047, 2049, 4095, 4096, 4097, 64 ** 3, 1_000_003, (1 << 22) - 1, 1 << 22,
-                               8_192_001])
+@pytest.mark.parametrize("m", [1, 31, 2047, 2048, 2049, 4095, 4096, 4097, 64 ** 3, 1_000_003, 1 << 21, (1 << 21) + 1,
+                               (1 << 22) - 1, 1 << 22, 8_192_001])
 def test_scan_matches_exclusive_prefix(m):
     """pbf_scan_exclusive_i32 on the shape of test/testPrefixSum.cpp:65-85
     (values rand()%16) and on ragged / large sizes; the total lands at out[m]."""
