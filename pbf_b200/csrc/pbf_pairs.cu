@@ -214,8 +214,8 @@ __device__ __forceinline__ void block_error_reduce(float e, unsigned long long* 
     }
 }
 
-// Neighbour entries in flight per thread and batch: four (two in the vorticity
-// pass, which gathers three float4s per entry).
+// Neighbour entries per thread and batch: four in every pass (V entries per
+// packed instruction, 4 / V instructions' worth of gathers issued together).
 template <int V> __host__ __device__ constexpr int batches() { return 4 / V; }
 
 // ---------------------------------------------------------------------------
