@@ -13,6 +13,11 @@ the launching stream after an L2 flush (a 256 MiB write); value = particles x K
 / sum of substep times, whole job (max over ranks). Under torchrun every rank
 runs its own replica of the scene (no data-path collective).
 
+e2e: the same K substeps through the public host-buffer call (pbf_step_host):
+step k copies the state the timed step k started from up from pinned host
+memory, uploads it, runs one substep and copies the positions back; beside it
+the same chain from device-resident inputs and the host link's rates.
+
 --impl reference times the reference's own CPU solver (src/solver.cpp built
 from its sources into oracle/_ref) on the host cores.
 """
