@@ -82,9 +82,11 @@ __global__ void __launch_bounds__(256, 8) k_hash(KParams p, const float4* __rest
 // bounded anyway and reports DEVERR_SCAN_TIMEOUT.
 // ---------------------------------------------------------------------------
 constexpr int SCAN_THREADS = 256;
-constexpr int SCAN_ITEMS = 32;
-constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr long long SCAN_SPIN_LIMIT = 1ll << 22;
+// Counts per thread: 32 (tiles of 8,192), or 64 (tiles of 16,384) above 2^22
+// counts, where half as many tiles shorten the look-back chains.
+constexpr int SCAN_LARGE_MIN = (1 << 22) + 1;
+__host__ __device__ constexpr int scan_items(int m) { return m >= SCAN_LARGE_MIN ? 64 : 32; }
 
 __device__ __forceinline__ void st_release_u64(unsigned long long* a, unsigned long long v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(a), "l"(v) : "memory");
@@ -97,11 +99,12 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 
 // VEC: cnt and out are 16-byte aligned; each lane moves four consecutive counts
 // per access (int4), four rounds of 128 per warp instead of sixteen of 32.
-template <bool VEC>
+template <bool VEC, int SCAN_ITEMS>
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, int* __restrict__ out, int m,
                                                        unsigned long long* __restrict__ status,
                                                        int* __restrict__ tile_counter, int* __restrict__ err,
                                                        int clear) {
+    constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
     __shared__ int s_tile;
     __shared__ int s_warp[SCAN_THREADS / 32];
     __shared__ int s_excl, s_tot;
@@ -110,7 +113,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
     __syncthreads();
     const int tile = s_tile;
 
-    // Warp w owns elements [tile * TILE + w * 512, +512) in rounds of consecutive
+    // Warp w owns elements [tile * TILE + w * 32 ITEMS, + 32 ITEMS) in rounds of consecutive
     // elements (coalesced: 32 counts per round, or 128 as int4 when VEC); each
     // round is scanned across the warp and carried into the next.
     const long long wbase = (long long)tile * SCAN_TILE + (long long)warp * (32 * SCAN_ITEMS);
@@ -628,29 +631,35 @@ void launch_hash(const KParams& p, bool predict_on, const float4* x, const float
     }
 }
 
-size_t scan_status_bytes(int m) {
-    const int tiles = (m + SCAN_TILE - 1) / SCAN_TILE;
-    return (size_t)tiles * sizeof(unsigned long long) + 16;
+static int scan_tiles(int m) {
+    const int tile = SCAN_THREADS * scan_items(m);
+    return (m + tile - 1) / tile;
+}
+
+size_t scan_status_bytes(int m) { return (size_t)scan_tiles(m) * sizeof(unsigned long long) + 16; }
+
+template <bool VEC>
+static void launch_scan_kernel(int* cnt, int* out, int m, unsigned long long* status, int* counter, int* err,
+                               int clear, cudaStream_t st) {
+    const int tiles = scan_tiles(m);
+    if (scan_items(m) == 64) k_scan<VEC, 64><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, clear);
+    else k_scan<VEC, 32><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, clear);
 }
 
 void launch_scan(int* cnt, int* out, int m, void* status_ws, int* err, cudaStream_t st) {
-    const int tiles = (m + SCAN_TILE - 1) / SCAN_TILE;
     unsigned long long* status = (unsigned long long*)status_ws;
-    int* counter = (int*)(status + tiles);
+    int* counter = (int*)(status + scan_tiles(m));
     cudaMemsetAsync(status_ws, 0, scan_status_bytes(m), st);
-    if (aligned16(cnt) && aligned16(out)) k_scan<true><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, 1);
-    else k_scan<false><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, 1);
+    if (aligned16(cnt) && aligned16(out)) launch_scan_kernel<true>(cnt, out, m, status, counter, err, 1, st);
+    else launch_scan_kernel<false>(cnt, out, m, status, counter, err, 1, st);
 }
 
 void launch_scan_const(const int* in, int* out, int m, void* status_ws, int* err, cudaStream_t st) {
-    const int tiles = (m + SCAN_TILE - 1) / SCAN_TILE;
     unsigned long long* status = (unsigned long long*)status_ws;
-    int* counter = (int*)(status + tiles);
+    int* counter = (int*)(status + scan_tiles(m));
     cudaMemsetAsync(status_ws, 0, scan_status_bytes(m), st);
-    if (aligned16(in) && aligned16(out))
-        k_scan<true><<<tiles, SCAN_THREADS, 0, st>>>(const_cast<int*>(in), out, m, status, counter, err, 0);
-    else
-        k_scan<false><<<tiles, SCAN_THREADS, 0, st>>>(const_cast<int*>(in), out, m, status, counter, err, 0);
+    if (aligned16(in) && aligned16(out)) launch_scan_kernel<true>(const_cast<int*>(in), out, m, status, counter, err, 0, st);
+    else launch_scan_kernel<false>(const_cast<int*>(in), out, m, status, counter, err, 0, st);
 }
 
 void launch_scatter(int n, const int* cell, const int* ticket, const int* cell_start, int* tmp, int* err,
