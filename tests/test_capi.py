@@ -85,6 +85,16 @@ def test_create_rejects_bad_extensions(field, value):
     assert rc == _lib.PBF_ERR_INVALID
 
 
+@pytest.mark.parametrize("m,tile", [(1, 8192), (8192, 8192), (8193, 8192), (1 << 22, 8192),
+                                    ((1 << 22) + 1, 16384), (16_777_216, 16384)])
+def test_scan_workspace_holds_one_status_word_per_tile(m, tile):
+    """The scan's workspace: one 8-byte status word per tile, the tile counter
+    and the error word; tiles of 8,192 counts up to 2^22 counts, of 16,384 above
+    (host arithmetic only, no GPU)."""
+    tiles = -(-m // tile)
+    assert lib().pbf_scan_workspace_bytes(m) == tiles * 8 + 16 + 16
+
+
 def test_null_handles_are_errors_not_crashes():
     L = lib()
     assert L.pbf_step(None, 1, None) == _lib.PBF_ERR_INVALID
