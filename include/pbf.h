@@ -177,6 +177,16 @@ int pbf_bind_position(pbf_solver* s, float* d_pos);
  * the captured substep graph `substeps` times on `stream`. */
 int pbf_step(pbf_solver* s, int substeps, void* stream);
 
+/* New SolverParameter values for the following substeps, as the reference's
+ * cudaPBFSolve(data, para) takes them on every call (kernels/cudaPBF.cu:50-115
+ * reads h, dt, iterations, restRho, epsilon, k, n, deltaq, c and the vorticity
+ * epsilon from para each time). para->nParticles must equal the solver's
+ * particle count. Unchanged values cost nothing; changed ones take effect from
+ * the next pbf_step, which captures its graph again, and the grid hash the next
+ * substep starts from is made again with them (stream-ordered on the stream of
+ * the last call). */
+int pbf_set_parameter(pbf_solver* s, const pbf_solver_parameter* para);
+
 /* One frame from and to host memory, asynchronous and pipelined across calls
  * (no reference counterpart; the host side of initCUDASolverDataBuffer's
  * copies and cudaPBFSolve in one call): copies pos and vel (AoS xyz float[3n];
@@ -190,6 +200,25 @@ int pbf_step(pbf_solver* s, int substeps, void* stream);
  * reading pos_out. */
 int pbf_step_host(pbf_solver* s, const float* pos, const float* vel, float* pos_out, int substeps, void* stream);
 int pbf_host_fence(pbf_solver* s, void* stream);
+
+/* Testing hook (host-side fault injection, no reference counterpart): the k-th
+ * device allocation of the next pbf_step_host staging set-up (1-based; four per
+ * set-up) fails as if the device were out of memory; 0 turns it off. A failed
+ * set-up returns PBF_ERR_ALLOC and leaves the handle as it was, so the next call
+ * sets the staging up again. */
+int pbf_debug_fail_staging_alloc(int k);
+
+/* Testing hook (failure injection on the device without a fault, no reference
+ * counterpart; the reference's CHECK_CUDA exits the process instead,
+ * kernels/cudaPBFSolver.cuh:5-10). Runs one production kernel with a wait that
+ * nothing will satisfy and a short limit: which = 0, the exclusive scan with a
+ * tile that never publishes its status (the look-back waits of its successors
+ * run out); which = 1, the warm-start network's forward kernel with nothing
+ * committed to its tensor-core barrier. The kernel records the expired wait in
+ * its error word, frees what it holds and returns; *error_bits receives the
+ * word (PBF_DEVERR_SCAN_TIMEOUT or PBF_DEVERR_MLP_TIMEOUT) and the call returns
+ * PBF_ERR_DEVICE, with the CUDA context still usable. Synchronises the device. */
+int pbf_debug_expire_wait(int which, int* error_bits);
 
 /* Changes the particle count of a single-scene solver to n (1 <= n <= the
  * nParticles it was created with); the next pbf_step captures its graph again
@@ -248,9 +277,11 @@ int pbf_graph_kernel_count(pbf_solver* s);
 int pbf_measure_density_error(pbf_solver* s, double* max_err, double* mean_err, void* stream);
 
 /* Exclusive scan of int32 with decoupled look-back (calculatePrefixSum +
- * addBlockSum, kernels/cudaPBFSolver.cu:42-96, for any n). d_out receives n + 1
- * ints (the total last). d_ws must hold pbf_scan_workspace_bytes(n) bytes.
- * The input is left unchanged. */
+ * addBlockSum, kernels/cudaPBFSolver.cu:42-96, for 1 <= n <= PBF_SCAN_MAX_COUNT;
+ * larger n is rejected with PBF_ERR_INVALID and pbf_scan_workspace_bytes returns
+ * 0 for it). d_out receives n + 1 ints (the total last). d_ws must hold
+ * pbf_scan_workspace_bytes(n) bytes. The input is left unchanged. */
+#define PBF_SCAN_MAX_COUNT (1 << 30)
 size_t pbf_scan_workspace_bytes(int n);
 int pbf_scan_exclusive_i32(const int* d_in, int* d_out, int n, void* d_ws, size_t ws_bytes, void* stream);
 

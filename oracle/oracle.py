@@ -52,6 +52,7 @@ def olib() -> C.CDLL:
         L.oracle_create.restype = C.c_void_p
         L.oracle_create.argtypes = [C.POINTER(OracleParams), C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.oracle_substep.argtypes = [C.c_void_p]
+        L.oracle_set_params.argtypes = [C.c_void_p, C.POINTER(OracleParams)]
         L.oracle_substep_adaptive.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int]
         L.oracle_build_only.argtypes = [C.c_void_p]
         L.oracle_get.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
@@ -132,6 +133,12 @@ class Oracle:
     def substep(self, count: int = 1) -> None:
         for _ in range(count):
             olib().oracle_substep(self._h)
+
+    def set_params(self, params: OracleParams) -> None:
+        """New parameter values for the following substeps (same grid and cap)."""
+        if olib().oracle_set_params(self._h, C.byref(params)) != 0:
+            raise ValueError("oracle_set_params: the grid or the neighbour cap changed")
+        self.params = params
 
     def substep_adaptive(self, tol: float, min_iterations: int, max_iterations: int) -> int:
         """One adaptive substep of the CUDA library (ext.adaptive): corrections until

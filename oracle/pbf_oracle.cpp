@@ -844,6 +844,22 @@ void* oracle_create(const oracle_params* p, int precision, int n, const float* p
     return h;
 }
 
+// New parameter values for the following substeps (the library's
+// pbf_set_parameter): the grid (dims, cell scale) and neighbour cap must stay.
+int oracle_set_params(void* hv, const oracle_params* p) {
+    Handle* h = (Handle*)hv;
+    if (!h || !p) return -1;
+    auto apply = [&](auto* sv) {
+        if (p->dims[0] != sv->p.dims[0] || p->dims[1] != sv->p.dims[1] || p->dims[2] != sv->p.dims[2] ||
+            p->max_nbr != sv->p.max_nbr)
+            return -1;
+        sv->p = *p;
+        sv->make_consts();
+        return 0;
+    };
+    return h->f ? apply(h->f) : apply(h->d);
+}
+
 int oracle_substep(void* hv) {
     Handle* h = (Handle*)hv;
     if (!h) return -1;

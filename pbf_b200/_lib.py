@@ -19,6 +19,11 @@ PBF_ERR_DEVICE = -4
 PBF_ERR_STATE = -5
 PBF_ERR_NONFINITE = -6
 
+PBF_DEVERR_SCAN_TIMEOUT = 1
+PBF_DEVERR_BAD_INDEX = 2
+PBF_DEVERR_NONFINITE = 4
+PBF_DEVERR_MLP_TIMEOUT = 8
+
 PBF_FLAG_CLAMP_C = 1
 PBF_FLAG_XSPH_RHO = 2
 PBF_FLAG_WALL_DENSITY = 4
@@ -116,7 +121,10 @@ _PROTOS = [
     ("pbf_download_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("pbf_step_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     ("pbf_host_fence", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pbf_debug_fail_staging_alloc", C.c_int, [C.c_int]),
+    ("pbf_debug_expire_wait", C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     ("pbf_resize", C.c_int, [C.c_void_p, C.c_int]),
+    ("pbf_set_parameter", C.c_int, [C.c_void_p, C.POINTER(SolverParameter)]),
     ("pbf_download_sorted_device", C.c_int, [C.c_void_p] + [C.c_void_p] * 5 + [C.c_void_p]),
     ("pbf_get_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("pbf_fetch", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),

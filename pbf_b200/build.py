@@ -45,16 +45,30 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+def reference_dir() -> str:
+    """Where the reference's source tree is on this machine, or "" when it is not:
+    $PBF_REFERENCE_DIR, else the build container's read-only checkout. The
+    reference is needed only to build the test checkers; a machine without it
+    uses the checkers built where it was present."""
+    for d in (os.environ.get("PBF_REFERENCE_DIR", ""), "/root/reference"):
+        if d and os.path.isdir(os.path.join(d, "src")) and os.path.isdir(os.path.join(d, "kernels")):
+            return d
+    return ""
+
+
 def build_oracle(verbose: bool = False) -> None:
-    """Test infrastructure: the CPU restatement, plus the reference checkers when
-    the reference sources are present on this machine."""
+    """Test infrastructure: the CPU restatement, plus the reference checkers (the
+    reference's CPU and CUDA solvers built from its sources, and the test program
+    that drives this library through the reference's own entry points) when the
+    reference sources are present on this machine."""
     odir = os.path.join(REPO, "oracle")
     targets = ["oracle"]
-    ref = os.environ.get("PBF_REFERENCE_DIR", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "src")):
-        targets += ["refcpu", "refgpu"]
-    subprocess.run(["make", "-s", "-C", odir, f"REF={ref}"] + targets, check=True,
-                   stdout=None if verbose else subprocess.DEVNULL)
+    ref = reference_dir()
+    args = ["make", "-s", "-C", odir]
+    if ref:
+        targets += ["refcpu", "refgpu", "refapp"]
+        args.append(f"REF={ref}")
+    subprocess.run(args + targets, check=True, stdout=None if verbose else subprocess.DEVNULL)
 
 
 def build(force: bool = False, verbose: bool = False) -> None:

@@ -5,6 +5,7 @@
 // cudaDeviceSynchronize round trips and two leaked host arrays per substep).
 // Here one substep is a CUDA graph captured once per handle and replayed.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -199,6 +200,30 @@ KParams make_kparams(const pbf_solver& s) {
     return k;
 }
 
+// Host-side fault injection for tests (pbf_debug_fail_staging_alloc): when
+// positive, the device allocation of pbf_step_host's staging with this 1-based
+// number fails as if the device were out of memory.
+std::atomic<int> g_fail_staging_alloc{0};
+
+cudaError_t staging_malloc(void** p, size_t bytes) {
+    if (g_fail_staging_alloc.load() > 0 && g_fail_staging_alloc.fetch_sub(1) == 1) return cudaErrorMemoryAllocation;
+    return cudaMalloc(p, bytes);
+}
+
+// Frees whatever part of a HostPipe exists (null members are skipped).
+void free_host_pipe(HostPipe* hp) {
+    if (!hp) return;
+    for (int b = 0; b < 2; ++b) {
+        if (hp->in[b]) cudaFree(hp->in[b]);
+        if (hp->out[b]) cudaFree(hp->out[b]);
+        for (cudaEvent_t e : {hp->in_ready[b], hp->in_free[b], hp->out_ready[b], hp->out_free[b]})
+            if (e) cudaEventDestroy(e);
+    }
+    if (hp->h2d) cudaStreamDestroy(hp->h2d);
+    if (hp->d2h) cudaStreamDestroy(hp->d2h);
+    delete hp;
+}
+
 template <typename T> int dalloc(T** p, size_t count) {
     if (count == 0) count = 1;
     cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
@@ -216,18 +241,8 @@ void free_all(pbf_solver* s) {
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->graph) cudaGraphDestroy(s->graph);
     if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
-    if (HostPipe* hp = s->hp) {
-        for (int b = 0; b < 2; ++b) {
-            if (hp->in[b]) cudaFree(hp->in[b]);
-            if (hp->out[b]) cudaFree(hp->out[b]);
-            for (cudaEvent_t e : {hp->in_ready[b], hp->in_free[b], hp->out_ready[b], hp->out_free[b]})
-                if (e) cudaEventDestroy(e);
-        }
-        if (hp->h2d) cudaStreamDestroy(hp->h2d);
-        if (hp->d2h) cudaStreamDestroy(hp->d2h);
-        delete hp;
-        s->hp = nullptr;
-    }
+    free_host_pipe(s->hp);
+    s->hp = nullptr;
     if (s->body_stream) cudaStreamDestroy(s->body_stream);
     for (auto& e : s->prof) {
         cudaEventDestroy(e.a);
@@ -786,19 +801,25 @@ int pbf_step_host(pbf_solver* s, const float* pos, const float* vel, float* pos_
     if (!s || !pos || !vel || !pos_out) return fail(PBF_ERR_INVALID, "null argument");
     if (substeps < 0) return fail(PBF_ERR_INVALID, "negative substep count");
     if (!s->hp) {
+        // built aside and attached only once every stream, buffer and event
+        // exists, so a failed set-up leaves the handle as it was and the next
+        // call tries again
         HostPipe* hp = new (std::nothrow) HostPipe();
         if (!hp) return fail(PBF_ERR_ALLOC, "host allocation failed");
-        s->hp = hp;
         const size_t n = s->capacity;
         cudaError_t e = cudaStreamCreateWithFlags(&hp->h2d, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&hp->d2h, cudaStreamNonBlocking);
         for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-            e = cudaMalloc(&hp->in[b], sizeof(float) * 6 * std::max<size_t>(n, 1));
-            if (e == cudaSuccess) e = cudaMalloc(&hp->out[b], sizeof(float) * 3 * std::max<size_t>(n, 1));
+            e = staging_malloc((void**)&hp->in[b], sizeof(float) * 6 * std::max<size_t>(n, 1));
+            if (e == cudaSuccess) e = staging_malloc((void**)&hp->out[b], sizeof(float) * 3 * std::max<size_t>(n, 1));
             for (cudaEvent_t* ev : {&hp->in_ready[b], &hp->in_free[b], &hp->out_ready[b], &hp->out_free[b]})
                 if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
         }
-        if (e != cudaSuccess) return fail(PBF_ERR_ALLOC, "pbf_step_host staging: %s", cudaGetErrorString(e));
+        if (e != cudaSuccess) {
+            free_host_pipe(hp);
+            return fail(PBF_ERR_ALLOC, "pbf_step_host staging: %s", cudaGetErrorString(e));
+        }
+        s->hp = hp;
     }
     HostPipe& hp = *s->hp;
     cudaStream_t st = (cudaStream_t)stream;
@@ -827,12 +848,82 @@ int pbf_step_host(pbf_solver* s, const float* pos, const float* vel, float* pos_
     return PBF_OK;
 }
 
+int pbf_debug_expire_wait(int which, int* error_bits) {
+    if (!error_bits) return fail(PBF_ERR_INVALID, "null argument");
+    if (which != 0 && which != 1) return fail(PBF_ERR_INVALID, "which must be 0 (scan) or 1 (tensor-core barrier)");
+    *error_bits = 0;
+    const int m = 3 * 8192;  // three scan tiles; 192 feature rows for the network
+    int *d_in = nullptr, *d_out = nullptr, *d_err = nullptr;
+    void* ws = nullptr;
+    uint16_t* w = nullptr;
+    float *b = nullptr, *feat = nullptr, *out = nullptr;
+    cudaError_t e = cudaMalloc(&d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(d_err, 0, sizeof(int));
+    if (e == cudaSuccess && which == 0) {
+        e = cudaMalloc(&d_in, sizeof(int) * m);
+        if (e == cudaSuccess) e = cudaMemset(d_in, 0, sizeof(int) * m);
+        if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(int) * (m + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&ws, scan_status_bytes(m));
+        // tile 0 never publishes; its successors give up after 4,096 polls
+        if (e == cudaSuccess) launch_scan_silent_tile(d_in, d_out, m, ws, d_err, 0, 4096, nullptr);
+    } else if (e == cudaSuccess) {
+        const int rows = 192;
+        e = cudaMalloc(&w, sizeof(uint16_t) * MLP_NUM_WEIGHTS);
+        if (e == cudaSuccess) e = cudaMemset(w, 0, sizeof(uint16_t) * MLP_NUM_WEIGHTS);
+        if (e == cudaSuccess) e = cudaMalloc(&b, sizeof(float) * MLP_NUM_BIASES);
+        if (e == cudaSuccess) e = cudaMemset(b, 0, sizeof(float) * MLP_NUM_BIASES);
+        if (e == cudaSuccess) e = cudaMalloc(&feat, sizeof(float) * MLP_IN * rows);
+        if (e == cudaSuccess) e = cudaMemset(feat, 0, sizeof(float) * MLP_IN * rows);
+        if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(float) * rows);
+        if (e == cudaSuccess && mlp_infer_uncommitted(w, b, feat, rows, out, 4096, d_err, nullptr))
+            e = cudaErrorLaunchFailure;
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(error_bits, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    for (void* p : {(void*)d_in, (void*)d_out, (void*)d_err, ws, (void*)w, (void*)b, (void*)feat, (void*)out})
+        if (p) cudaFree(p);
+    if (e != cudaSuccess) return fail(PBF_ERR_CUDA, "pbf_debug_expire_wait: %s", cudaGetErrorString(e));
+    if (*error_bits) return fail(PBF_ERR_DEVICE, "kernel error bits 0x%x", *error_bits);
+    return PBF_OK;
+}
+
+int pbf_debug_fail_staging_alloc(int k) {
+    if (k < 0) return fail(PBF_ERR_INVALID, "k must be >= 0");
+    g_fail_staging_alloc.store(k);
+    return PBF_OK;
+}
+
 int pbf_host_fence(pbf_solver* s, void* stream) {
     if (!s) return fail(PBF_ERR_INVALID, "null handle");
     if (!s->hp || s->hp->calls == 0) return PBF_OK;
     // copies of one direction complete in call order; the last copy-out comes
     // after its call's copy-in
     CK(cudaStreamWaitEvent((cudaStream_t)stream, s->hp->out_free[(s->hp->calls - 1) & 1], 0));
+    return PBF_OK;
+}
+
+int pbf_set_parameter(pbf_solver* s, const pbf_solver_parameter* para) {
+    if (!s || !para) return fail(PBF_ERR_INVALID, "null argument");
+    if (para->nParticles != s->n)
+        return fail(PBF_ERR_INVALID, "nParticles (%d) differs from the solver's %d particles", para->nParticles, s->n);
+    const int rc = validate(para, s->grid_space, s->boundary, &s->ext);
+    if (rc) return rc;
+    if (std::memcmp(para, &s->para, sizeof *para) == 0) return PBF_OK;
+    s->para = *para;
+    s->kp = make_kparams(*s);
+    if (s->exec) {  // constants and the iteration count live in the captured graph
+        cudaGraphExecDestroy(s->exec);
+        s->exec = nullptr;
+    }
+    if (s->uploaded) {
+        // The next substep's grid hash (prediction with dt and gravity, cell keys
+        // with h) was made with the old values; make it again from the state.
+        cudaStream_t st = s->last_stream;
+        CK(cudaMemsetAsync(s->cnt, 0, sizeof(int) * (size_t)s->nkeys, st));
+        launch_hash(s->kp, true, s->Sx, s->Sv, s->cell, s->ticket, s->cnt, &s->dstats->err, st);
+        CK(cudaGetLastError());
+    }
     return PBF_OK;
 }
 
@@ -1176,13 +1267,14 @@ int pbf_tc_gemm_bf16(const void* d_a, const void* d_b, float* d_d, int n, int k,
 }
 
 size_t pbf_scan_workspace_bytes(int n) {
-    if (n < 0) return 0;
+    if (n <= 0 || n > PBF_SCAN_MAX_COUNT) return 0;
     return scan_status_bytes(n) + 16;
 }
 
 int pbf_scan_exclusive_i32(const int* d_in, int* d_out, int n, void* d_ws, size_t ws_bytes, void* stream) {
     if (!d_in || !d_out || !d_ws) return fail(PBF_ERR_INVALID, "null argument");
     if (n <= 0) return fail(PBF_ERR_INVALID, "n must be positive");
+    if (n > PBF_SCAN_MAX_COUNT) return fail(PBF_ERR_INVALID, "n exceeds the scan's maximum of 2^30 counts");
     if (ws_bytes < pbf_scan_workspace_bytes(n)) return fail(PBF_ERR_INVALID, "workspace too small");
     cudaStream_t st = (cudaStream_t)stream;
     int* err = (int*)((char*)d_ws + scan_status_bytes(n));

@@ -99,11 +99,13 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 
 // VEC: cnt and out are 16-byte aligned; each lane moves four consecutive counts
 // per access (int4), four rounds of 128 per warp instead of sixteen of 32.
+// silent_tile >= 0 (the failure-injection test only): that tile publishes no
+// status, so its successors' look-back waits run out after spin_limit polls.
 template <bool VEC, int SCAN_ITEMS>
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, int* __restrict__ out, int m,
                                                        unsigned long long* __restrict__ status,
                                                        int* __restrict__ tile_counter, int* __restrict__ err,
-                                                       int clear) {
+                                                       int clear, int silent_tile, long long spin_limit) {
     constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
     __shared__ int s_tile;
     __shared__ int s_warp[SCAN_THREADS / 32];
@@ -181,10 +183,11 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
         const int total = __shfl_sync(0xffffffffu, wi, SCAN_THREADS / 32 - 1);
         // decoupled look-back
         int excl = 0;
+        const bool publish = tile != silent_tile;
         if (tile == 0) {
-            if (lane == 0) st_release_u64(&status[0], (2ull << 32) | (unsigned)total);
+            if (lane == 0 && publish) st_release_u64(&status[0], (2ull << 32) | (unsigned)total);
         } else {
-            if (lane == 0) st_release_u64(&status[tile], (1ull << 32) | (unsigned)total);
+            if (lane == 0 && publish) st_release_u64(&status[tile], (1ull << 32) | (unsigned)total);
             int pos = tile - 1;  // highest tile not yet folded in
             bool done = false;
             while (!done) {
@@ -194,7 +197,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
                     long long spins = 0;
                     s = ld_acquire_u64(&status[look]);
                     while ((s >> 32) == 0ull) {
-                        if (++spins > SCAN_SPIN_LIMIT) {
+                        if (++spins > spin_limit) {
                             atomicOr(err, DEVERR_SCAN_TIMEOUT);
                             s = 2ull << 32;  // give up: treat as prefix 0 so the tile finishes
                             break;
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(int* __restrict__ cnt, in
                 if (prefix_mask) done = true;
                 else pos -= 32;
             }
-            if (lane == 0) st_release_u64(&status[tile], (2ull << 32) | (unsigned)(excl + total));
+            if (lane == 0 && publish) st_release_u64(&status[tile], (2ull << 32) | (unsigned)(excl + total));
         }
         if (lane == 0) {
             s_excl = excl;
@@ -631,19 +634,25 @@ void launch_hash(const KParams& p, bool predict_on, const float4* x, const float
     }
 }
 
+// tile count in 64-bit arithmetic (m + tile - 1 would overflow an int near INT_MAX)
 static int scan_tiles(int m) {
-    const int tile = SCAN_THREADS * scan_items(m);
-    return (m + tile - 1) / tile;
+    const long long tile = (long long)SCAN_THREADS * scan_items(m);
+    return (int)(((long long)m + tile - 1) / tile);
 }
 
 size_t scan_status_bytes(int m) { return (size_t)scan_tiles(m) * sizeof(unsigned long long) + 16; }
 
 template <bool VEC>
 static void launch_scan_kernel(int* cnt, int* out, int m, unsigned long long* status, int* counter, int* err,
-                               int clear, cudaStream_t st) {
+                               int clear, cudaStream_t st, int silent_tile = -1,
+                               long long spin_limit = SCAN_SPIN_LIMIT) {
     const int tiles = scan_tiles(m);
-    if (scan_items(m) == 64) k_scan<VEC, 64><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, clear);
-    else k_scan<VEC, 32><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, clear);
+    if (scan_items(m) == 64)
+        k_scan<VEC, 64><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, clear, silent_tile,
+                                                         spin_limit);
+    else
+        k_scan<VEC, 32><<<tiles, SCAN_THREADS, 0, st>>>(cnt, out, m, status, counter, err, clear, silent_tile,
+                                                         spin_limit);
 }
 
 void launch_scan(int* cnt, int* out, int m, void* status_ws, int* err, cudaStream_t st) {
@@ -660,6 +669,14 @@ void launch_scan_const(const int* in, int* out, int m, void* status_ws, int* err
     cudaMemsetAsync(status_ws, 0, scan_status_bytes(m), st);
     if (aligned16(in) && aligned16(out)) launch_scan_kernel<true>(const_cast<int*>(in), out, m, status, counter, err, 0, st);
     else launch_scan_kernel<false>(const_cast<int*>(in), out, m, status, counter, err, 0, st);
+}
+
+void launch_scan_silent_tile(const int* in, int* out, int m, void* status_ws, int* err, int silent_tile,
+                             long long spin_limit, cudaStream_t st) {
+    unsigned long long* status = (unsigned long long*)status_ws;
+    int* counter = (int*)(status + scan_tiles(m));
+    cudaMemsetAsync(status_ws, 0, scan_status_bytes(m), st);
+    launch_scan_kernel<false>(const_cast<int*>(in), out, m, status, counter, err, 0, st, silent_tile, spin_limit);
 }
 
 void launch_scatter(int n, const int* cell, const int* ticket, const int* cell_start, int* tmp, int* err,

@@ -17,6 +17,10 @@ size_t scan_status_bytes(int m);
 void launch_scan(int* cnt, int* out, int m, void* status_ws, int* err, cudaStream_t st);
 // same scan, input left unchanged
 void launch_scan_const(const int* in, int* out, int m, void* status_ws, int* err, cudaStream_t st);
+// failure injection (tests): tile silent_tile publishes no status and the
+// look-back gives up after spin_limit polls (input left unchanged)
+void launch_scan_silent_tile(const int* in, int* out, int m, void* status_ws, int* err, int silent_tile,
+                             long long spin_limit, cudaStream_t st);
 void launch_scatter(int n, const int* cell, const int* ticket, const int* cell_start, int* tmp, int* err,
                     cudaStream_t st);
 void launch_reorder(const KParams& p, bool predict_on, const float4* x, const float4* v, const int* perm,

@@ -162,11 +162,14 @@ __device__ __forceinline__ void put_row64(uint8_t* s, int row, const float (&v)[
 // thread leaves the tile loop together). On an expired wait the error bit is
 // set and a second bounded wait gives MMAs still in flight time to finish
 // before the caller frees TMEM.
-__device__ __forceinline__ bool wait_mma(uint64_t* mbar, uint32_t& phase, int* err) {
-    bool ok = mbar_wait(mbar, phase);
+constexpr long long MBAR_WAIT_LIMIT = 1ll << 24;  // polls of one bounded wait
+
+__device__ __forceinline__ bool wait_mma(uint64_t* mbar, uint32_t& phase, int* err,
+                                         long long limit = MBAR_WAIT_LIMIT) {
+    bool ok = mbar_wait(mbar, phase, limit);
     if (!ok) {
         if ((threadIdx.x & 31) == 0) atomicOr(err, DEVERR_MLP_TIMEOUT);
-        mbar_wait(mbar, phase);
+        mbar_wait(mbar, phase, limit);
     }
     phase ^= 1u;
     ok = __syncthreads_and(ok) != 0;
@@ -203,6 +206,10 @@ struct FwdIO {
     float* gb;                                 // gradient of b4 written here
     float* loss;
     int* err;
+    // failure injection (the bounded-wait test only): no MMA is issued or
+    // committed, so every wait on the barrier runs out after wait_limit polls
+    int no_commit = 0;
+    long long wait_limit = MBAR_WAIT_LIMIT;
 };
 
 constexpr int FWD_SW1 = 0;                              // [64 x 16]   2 KB
@@ -265,11 +272,11 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
         }
         // ---- layer 1: TMEM cols [0, 64)
         sync_for_mma();
-        if (t == 0) {
+        if (t == 0 && !io.no_commit) {
             gemm_issue(tbase, smem + FWD_SX, smem + FWD_SW1, 64, 16, 0);
             commit(&mbar);
         }
-        if (!wait_mma(&mbar, phase, io.err)) { alive = false; break; }
+        if (!wait_mma(&mbar, phase, io.err, io.wait_limit)) { alive = false; break; }
 #pragma unroll 1
         for (int c = 0; c < 4; ++c) {
             float v[16];
@@ -296,11 +303,11 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
         }
         // ---- layer 2: TMEM cols [64, 128)
         sync_for_mma();
-        if (t == 0) {
+        if (t == 0 && !io.no_commit) {
             gemm_issue(tbase + 64, smem + FWD_SH1, smem + FWD_SW2, 64, 64, 0);
             commit(&mbar);
         }
-        if (!wait_mma(&mbar, phase, io.err)) { alive = false; break; }
+        if (!wait_mma(&mbar, phase, io.err, io.wait_limit)) { alive = false; break; }
 #pragma unroll 1
         for (int c = 0; c < 4; ++c) {
             float v[16];
@@ -328,11 +335,11 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
         // ---- layer 3: TMEM cols [0, 64) again (layer 1's values were consumed
         // before layer 2 was issued), then the output layer on CUDA cores
         sync_for_mma();
-        if (t == 0) {
+        if (t == 0 && !io.no_commit) {
             gemm_issue(tbase, smem + FWD_SH2, smem + FWD_SW3, 64, 64, 0);
             commit(&mbar);
         }
-        if (!wait_mma(&mbar, phase, io.err)) { alive = false; break; }
+        if (!wait_mma(&mbar, phase, io.err, io.wait_limit)) { alive = false; break; }
         float y = sb[B4_OFF];
         float* h3f = reinterpret_cast<float*>(smem + FWD_SH3F) + t * 64;
 #pragma unroll 1
@@ -576,6 +583,26 @@ int mlp_infer(const uint16_t* w_bf16, const float* b, const float* feat, int n, 
     const int tiles = (n + TILE - 1) / TILE;
     const int grid = tiles < 4 * sm_count() ? tiles : 4 * sm_count();
     k_mlp_fwd<false><<<grid, 128, FWD_SMEM_INFER, st>>>(io);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int mlp_infer_uncommitted(const uint16_t* w_bf16, const float* b, const float* feat, int n, float* out,
+                          long long wait_limit, int* err, cudaStream_t st) {
+    if (n <= 0) return 0;
+    if (cudaFuncSetAttribute(k_mlp_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM_INFER) !=
+        cudaSuccess)
+        return -1;
+    FwdIO io{};
+    io.w = w_bf16;
+    io.b = b;
+    io.feat = feat;
+    io.n = n;
+    io.out = out;
+    io.err = err;
+    io.no_commit = 1;
+    io.wait_limit = wait_limit;
+    const int tiles = (n + TILE - 1) / TILE;
+    k_mlp_fwd<false><<<tiles, 128, FWD_SMEM_INFER, st>>>(io);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

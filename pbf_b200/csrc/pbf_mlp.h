@@ -43,6 +43,10 @@ int tc_gemm_bf16(const void* A, const void* B, float* D, int N, int K, int* err,
 // to at most clamp times its magnitude.
 int mlp_infer(const uint16_t* w_bf16, const float* b, const float* feat, int n, float* out, float4* q,
               float* lam_acc, float clamp, int* err, cudaStream_t st);
+// failure injection (tests): the same kernel with no MMA committed to its
+// barrier, each wait limited to wait_limit polls
+int mlp_infer_uncommitted(const uint16_t* w_bf16, const float* b, const float* feat, int n, float* out,
+                          long long wait_limit, int* err, cudaStream_t st);
 
 struct MlpTrainer;
 MlpTrainer* mlp_trainer_create(int max_batch, const float* w32, const float* b32);

@@ -84,6 +84,14 @@ class SlabGeometry:
         if halo_h is None:
             halo_h = 2 * int(para.iterations) + 4
         self.halo = int(math.ceil(halo_h / float(ext.cell_scale) - 1e-9))
+        # cell columns a result depends on (lambda and the correction reach h per
+        # Jacobi iteration, curl and vorticity h each), and what the halo leaves
+        # beyond that for motion within a substep
+        self.reach = int(math.ceil((2 * int(para.iterations) + 2) / float(ext.cell_scale) - 1e-9))
+        self.margin = self.halo - self.reach
+        if self.margin < 1:
+            raise ValueError(f"a halo of {self.halo} cell columns leaves no margin beyond the reach of "
+                             f"{self.reach} columns")
         nx = self.dims[0]
         self.edges = [round(r * nx / nslabs) for r in range(nslabs + 1)]
         self.nslabs = nslabs
@@ -148,7 +156,30 @@ class SlabRank:
         pos, vel, ids, key, rank = self.engine.run(local.pos.contiguous(), local.vel.contiguous())
         res = Part(pos, vel, local.gid[ids.long()], key, rank)
         keep = (self.geom.owner(pos) == self.r).nonzero().squeeze(1)
+        self.check_ghost_zone(local.pos[ids.long()], pos, keep)
         self.own = res.take(keep)
+
+    def check_ghost_zone(self, start, end, keep):
+        """The ghost zone is exact only while no particle moves farther than the
+        halo's margin (halo - reach cell columns) along x in one substep: a faster
+        one could start outside every halo and end in a neighbourhood, or a kept
+        particle could have started too deep in the halo for its neighbourhood to
+        be complete. Every rank checks the particles it computed (each particle
+        is owned, so computed completely, by some rank), and raises instead of
+        returning a state that would differ from the single-domain solver."""
+        g, r = self.geom, self.r
+        x0, _ = g.cells(start)
+        x1, _ = g.cells(end)
+        moved = int((x1 - x0).abs().max().item()) if x0.numel() else 0
+        if moved > g.margin:
+            raise RuntimeError(f"slab {r}: a particle moved {moved} cell columns in one substep, more than the "
+                               f"ghost zone's margin of {g.margin}; use a wider halo (halo_h) or a smaller dt")
+        if keep.numel():
+            k0 = x0[keep]
+            lo, hi = g.edges[r] - g.margin, g.edges[r + 1] + g.margin
+            if bool(((k0 < lo) | (k0 >= hi)).any()):
+                raise RuntimeError(f"slab {r}: a particle it keeps started deeper in the halo than the margin of "
+                                   f"{g.margin} cell columns, so its neighbourhood was incomplete")
 
 
 class SlabGroup:

@@ -125,6 +125,12 @@ class Solver:
     def step(self, substeps: int = 1, stream=None) -> None:
         check(lib().pbf_step(self._h, int(substeps), _stream_handle(stream)))
 
+    def set_parameter(self, para: SolverParameter) -> None:
+        """New SolverParameter values for the following substeps (pbf_set_parameter);
+        nParticles must stay the same."""
+        check(lib().pbf_set_parameter(self._h, C.byref(para)))
+        self.para = para
+
     def build_grid(self, stream=None) -> None:
         check(lib().pbf_build_grid(self._h, _stream_handle(stream)))
 
@@ -291,6 +297,10 @@ def initCUDASolverDataBuffer(position: np.ndarray, velocity: np.ndarray, para: S
 
 
 def cudaPBFSolve(data: Solver, para: Optional[SolverParameter] = None) -> None:
+    """One substep; like the reference (kernels/cudaPBF.cu:50-115) it takes the
+    parameters of this call, so changed values apply from this substep on."""
+    if para is not None:
+        data.set_parameter(para)
     data.step(1)
 
 

@@ -106,10 +106,40 @@ def test_null_handles_are_errors_not_crashes():
     assert L.pbf_scan_exclusive_i32(None, None, 4, None, 0, None) == _lib.PBF_ERR_INVALID
 
 
-REF = os.environ.get("PBF_REFERENCE_DIR", "/root/reference")
+def test_test_hooks_validate_on_the_host():
+    """The failure-injection hooks reject bad arguments before touching a GPU."""
+    L = lib()
+    bits = C.c_int(0)
+    assert L.pbf_debug_expire_wait(2, C.byref(bits)) == _lib.PBF_ERR_INVALID
+    assert L.pbf_debug_expire_wait(0, None) == _lib.PBF_ERR_INVALID
+    assert L.pbf_debug_fail_staging_alloc(-1) == _lib.PBF_ERR_INVALID
+    assert L.pbf_debug_fail_staging_alloc(0) == _lib.PBF_OK
 
 
-@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "include")), reason="reference headers not present")
+@pytest.mark.parametrize("m", [(1 << 30) + 1, 2**31 - 1])
+def test_scan_rejects_counts_beyond_its_limit(m):
+    """Counts above PBF_SCAN_MAX_COUNT (2^30) are refused on the host: no
+    workspace size, PBF_ERR_INVALID from the scan (tile arithmetic in 64 bits)."""
+    L = lib()
+    assert L.pbf_scan_workspace_bytes(m) == 0
+    assert L.pbf_scan_exclusive_i32(C.c_void_p(16), C.c_void_p(16), m, C.c_void_p(16), 1 << 20, None) == \
+        _lib.PBF_ERR_INVALID
+    tiles = -(-(1 << 30) // 16384)
+    assert L.pbf_scan_workspace_bytes(1 << 30) == tiles * 8 + 16 + 16
+
+
+def test_set_parameter_validates_on_the_host():
+    L = lib()
+    p = SolverParameter()
+    assert L.pbf_set_parameter(None, C.byref(p)) == _lib.PBF_ERR_INVALID
+
+
+from pbf_b200.build import reference_dir  # noqa: E402
+
+REF = reference_dir()
+
+
+@pytest.mark.skipif(not REF, reason="reference headers not present")
 def test_reference_shim_exports_the_reference_symbols(tmp_path):
     """reference_shim.cpp compiles against the reference's own headers and
     defines the same (mangled) functions the reference's kernels/cudaPBF.cu does."""

@@ -365,3 +365,35 @@ def test_step_host_pipelined_frames():
     stream.synchronize()
     for k in range(4):
         assert bits_equal(outs[k].numpy(), want[k % 2]), k
+
+
+@pytest.mark.parametrize("fail_at", [1, 2, 4])
+def test_step_host_staging_failure_leaves_the_handle_retryable(fail_at):
+    """A staging allocation of pbf_step_host that fails (injected on the host)
+    returns PBF_ERR_ALLOC and attaches nothing; the next call sets the staging
+    up again and gives the positions of a plain upload, step and download."""
+    import torch
+    from pbf_b200._lib import PBF_ERR_ALLOC, check, lib
+    sc = scenes.dam_break(12, (40, 20, 20), stable=True)
+    s = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext())
+    ref = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext())
+    ref.upload(sc.pos, sc.vel)
+    ref.step(1)
+    want = ref.download()[0]
+    pos = torch.from_numpy(np.ascontiguousarray(sc.pos, np.float32)).pin_memory()
+    vel = torch.from_numpy(np.ascontiguousarray(sc.vel, np.float32)).pin_memory()
+    out = torch.zeros((sc.n, 3), dtype=torch.float32).pin_memory()
+    stream = torch.cuda.Stream()
+    check(lib().pbf_debug_fail_staging_alloc(fail_at))
+    try:
+        with pytest.raises(PBFError) as e:
+            s.step_host(pos, vel, out, 1, stream)
+        assert e.value.code == PBF_ERR_ALLOC
+    finally:
+        check(lib().pbf_debug_fail_staging_alloc(0))
+    s.step_host(pos, vel, out, 1, stream)
+    s.host_fence(stream)
+    stream.synchronize()
+    assert bits_equal(out.numpy(), want)
+    s.close()
+    ref.close()

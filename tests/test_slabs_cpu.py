@@ -133,3 +133,20 @@ def test_two_ranks_match_single_domain_bitexact():
     want_v[perm] = o.get("v").astype(np.float32)
     assert np.array_equal(pos.view(np.uint32), want_x.view(np.uint32))
     assert np.array_equal(vel.view(np.uint32), want_v.view(np.uint32))
+
+
+def test_fast_particle_beyond_the_ghost_zone_is_an_error():
+    """A particle that moves farther along x in one substep than the halo's
+    margin (halo - reach) could leave a neighbourhood incomplete; the slab step
+    raises instead of returning a state that differs from the single domain."""
+    sc = slab_scene(iterations=2)
+    g = slabs.SlabGeometry(sc.para, sc.grid_space, sc.ext(), 2)
+    assert g.reach == 6 and g.margin == 2
+    vel = sc.vel.copy()
+    vel[0, 0] = 100.0  # 100 * dt = 0.83 = 8 cell columns in one substep
+    group = slabs.SlabGroup(g, [OracleEngine(sc), OracleEngine(sc)])
+    group.load(torch.from_numpy(sc.pos), torch.from_numpy(vel))
+    with pytest.raises(RuntimeError, match="cell columns"):
+        group.step(1)
+    with pytest.raises(ValueError):
+        slabs.SlabGeometry(sc.para, sc.grid_space, sc.ext(), 2, halo_h=6)  # no margin beyond the reach
