@@ -112,6 +112,17 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def measure_fp32_peaks() -> dict:
+    """Measured FP32 FMA throughput (TFLOP/s) of this GPU, scalar and packed f32x2."""
+    import ctypes as C
+
+    from pbf_b200._lib import check, lib
+    sc, pk = C.c_double(), C.c_double()
+    check(lib().pbf_measure_fp32_peak(C.byref(sc), C.byref(pk)))
+    return {"scalar_tflops": round(sc.value, 2), "f32x2_tflops": round(pk.value, 2),
+            "best": max(sc.value, pk.value)}
+
+
 def link_rates(pin_pos, pin_vel, d_pos, d_vel, out_h, d_out, stream, reps: int = 10) -> dict:
     """Host link rates of one step's copies on `stream`: positions and velocities
     up (24 B per particle), positions down (12 B), and both directions at once
@@ -281,13 +292,15 @@ def run_b200(args) -> int:
         tuned = {"cell_scale": args.cell_scale, "block_size": args.block_size, "pair_lanes": args.pair_lanes,
                  "table": "fixed on the command line"}
     else:
-        tuned = autotune.tune([sc], iterations=4)
+        # timed over the substeps the benchmark times (after its warm-up)
+        tuned = autotune.tune([sc], iterations=4, warm=max(args.warmup, 3), substeps=min(max(args.steps, 4), 10))
     ext_kw = dict(grid_dims=autotune.dims_for_scale(sc.ext_overrides["grid_dims"], tuned["cell_scale"]),
                   **autotune.ext_for(tuned))
     solver = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(**ext_kw))
     solver.upload(sc.pos, sc.vel)
     kernels = solver.kernel_count()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    fp32_peaks = measure_fp32_peaks()
 
     for _ in range(max(args.warmup, 3)):
         solver.step(1, stream)
@@ -421,7 +434,7 @@ def run_b200(args) -> int:
     alg_bytes = ALG_BYTES[dom] * n
     achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
     traffic = load_traffic(dom)
-    fp32_peak = 148 * 128 * 2 * (mp.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    fp32_peak, fp32_kind = fp32_peaks["best"], "measured (FMA probe: pbf_measure_fp32_peak, best of scalar and f32x2)"
     flops = ALG_FLOPS_PER_PAIR.get(dom, 0) * pairs
     step_bytes = (283.8 + 44 * 4) * n
     clocks = clk.summary()
@@ -445,7 +458,7 @@ def run_b200(args) -> int:
                      "alg_bytes_per_launch": alg_bytes, "launch_ms": launch_ms},
         "roofline_fp32": {"kernel": dom, "achieved": flops / (launch_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
                           "peak": fp32_peak, "frac": flops / (launch_ms * 1e-3) / 1e12 / fp32_peak,
-                          "peak_kind": "nominal 148 SM x 128 lanes x 2 at sm_max_mhz", "pairs": pairs},
+                          "peak_kind": fp32_kind, "probe": fp32_peaks, "pairs": pairs},
         "roofline_step": {"alg_bytes_per_step": step_bytes, "achieved_gbs": step_bytes / (tot_s / args.steps) / 1e9,
                           "frac_hbm": step_bytes / (tot_s / args.steps) / 1e9 / hbm_peak},
         "stages_ms": {k: round(v, 5) for k, v in stages.items()},
@@ -458,6 +471,8 @@ def run_b200(args) -> int:
         "clocks": clocks,
     }
     legs = set(args.legs.split(","))
+    if legs & {"all", "sweep"}:
+        out["sweep"] = measure_sweep(args, flush, stream)
     if legs & {"all", "render"}:
         out["render"] = measure_render(args, solver, sc, stream)
     if legs & {"all", "batched", "learned", "large"}:
@@ -491,7 +506,7 @@ def measure_batched(args, rank, world, dev, flush, stream, barrier, max_over_ran
     scs = scenes.config2(seed=0)
     parts = multigpu.assign_scenes([s.n for s in scs], world)
     mine = [scs[i] for i in parts[rank]]
-    tuned = autotune.tune(mine, iterations=4)
+    tuned = autotune.tune(mine, iterations=4, warm=max(args.warmup, 3), substeps=min(max(args.steps, 4), 10))
     para, descs, ov, pos, vel = scenes.batch_inputs(mine, iterations=4)
     for d in descs:
         d["grid_dims"] = autotune.dims_for_scale(d["grid_dims"], tuned["cell_scale"])
@@ -682,6 +697,69 @@ def measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, wei
     return out
 
 
+def measure_sweep(args, flush, stream) -> dict:
+    """Max density error against Jacobi iterations: for the 32,768- and
+    262,144-particle dam breaks and the 64-scene batch, each iteration count
+    (and the adaptive loop at 1 % with a cap of 64) runs its own trajectory from
+    the initial state: W untimed substeps, then K timed ones with the one-sided
+    error measured in FP64 after each. Rows: [iterations, ms per substep,
+    max error over the timed substeps, mean error, corrections per substep]."""
+    import torch
+
+    from pbf_b200 import BatchSolver, Solver, autotune, scenes
+    out = {"launch": {"cell_scale": 0.5, "block_size": 256, "pair_lanes": 2},
+           "columns": ["iterations", "ms_per_substep", "max_error", "mean_error", "corrections_per_substep"]}
+    counts = (2, 4, 8, 16, 32, 64)
+
+    def make(kind, iters, **kw):
+        lk = dict(cell_scale=0.5, block_size=256, pair_lanes=2, **kw)
+        if kind == "batch":
+            scs = scenes.config2(seed=0, iterations=iters)
+            para, descs, ov, pos, vel = scenes.batch_inputs(scs, iterations=iters)
+            for d in descs:
+                d["grid_dims"] = autotune.dims_for_scale(d["grid_dims"], 0.5)
+            ov.update(lk)
+            s = BatchSolver(para, descs, scenes.default_ext(**ov))
+        else:
+            sc = scenes.config0(iterations=iters) if kind == "config0" else scenes.config1(iterations=iters)
+            s = Solver(sc.para, sc.grid_space, sc.boundary,
+                       sc.ext(grid_dims=autotune.dims_for_scale(sc.ext_overrides["grid_dims"], 0.5), **lk))
+            pos, vel = sc.pos, sc.vel
+        s.upload(pos, vel)
+        return s
+
+    def run(s):
+        s.step(max(args.warmup, 3), stream)
+        before = s.stats()["total_iterations"]
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        errs = []
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            s.step(1, stream)
+            ev[k][1].record(stream)
+            errs.append(s.measure_density_error(stream))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+        corr = (s.stats()["total_iterations"] - before) / args.steps
+        return [round(ms, 4), round(max(e[0] for e in errs), 5), round(statistics.mean(e[1] for e in errs), 6),
+                round(corr, 2)]
+
+    for kind in ("config0", "config1", "batch"):
+        rows = []
+        for it in counts:
+            s = make(kind, it)
+            rows.append([it] + run(s))
+            s.close()
+        s = make(kind, 1, adaptive=1, density_tol=0.01, max_iterations=64, measure_error=1)
+        rows.append(["adaptive 1% (cap 64)"] + run(s))
+        s.close()
+        out[kind] = rows
+    reached = [(k, r[0], r[1]) for k in ("config0", "config1", "batch") for r in out[k] if r[2] <= 0.01]
+    out["reaches_1pct"] = [{"workload": k, "iterations": it, "ms_per_substep": ms} for k, it, ms in reached]
+    return out
+
+
 def membound_table(stages: dict, n: int, nkeys: int, peak: float) -> dict:
     """Achieved bandwidth of the HBM-bound kernels from per-launch stage times (ms)."""
     out = {}
@@ -738,8 +816,8 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--legs", default="all",
-                    help="comma list of legs after the single-scene one: all, batched, learned, large, cpu, render "
-                         "(main = the single-scene leg alone)")
+                    help="comma list of legs after the single-scene one: all, sweep, batched, learned, large, cpu, "
+                         "render (main = the single-scene leg alone)")
     ap.add_argument("--pair-lanes", type=int, default=0, help="with --cell-scale and --block-size: skip the "
                     "autotuner of the single-scene leg and use these launch settings")
     ap.add_argument("--cell-scale", type=float, default=0.0)

@@ -89,7 +89,14 @@ typedef struct pbf_ext_params {
     int pair_lanes;      /* threads sharing one particle's neighbour sums: 1, 2, 4 or 8 (default 2;
                             0 = 2). Lane t takes list entries t, t+L, ...; lane sums are combined
                             pairwise, so the value changes the FP32 summation order */
-    int reserved[3];
+    int persistent;      /* 1: each neighbour pass (search, lambda, dp, curl, vorticity) is one
+                            persistent launch: the blocks resident at once stride over all
+                            scenes' tiles of slots (default 0: one block per tile). Same results */
+    int warm_unfused;    /* 1: the warm start's feature pass and network as two launches with the
+                            features through HBM (default 0: one fused launch, the features go
+                            from the feature pass to the tensor cores through shared memory).
+                            Same results; kept for measurement */
+    int reserved[1];
 } pbf_ext_params;
 
 typedef struct pbf_stats {
@@ -219,6 +226,13 @@ int pbf_debug_fail_staging_alloc(int k);
  * word (PBF_DEVERR_SCAN_TIMEOUT or PBF_DEVERR_MLP_TIMEOUT) and the call returns
  * PBF_ERR_DEVICE, with the CUDA context still usable. Synchronises the device. */
 int pbf_debug_expire_wait(int which, int* error_bits);
+
+/* Measured FP32 fused multiply-add throughput of the current device in TFLOP/s
+ * (no reference counterpart): scalar FFMA and packed two-lane f32x2 FMA chains,
+ * 8 per thread on 8 blocks of 256 per SM, best of three CUDA-event-timed
+ * launches. The denominator the neighbour passes' FP32 rate is reported
+ * against. Synchronises the device. */
+int pbf_measure_fp32_peak(double* scalar_tflops, double* packed_tflops);
 
 /* Changes the particle count of a single-scene solver to n (1 <= n <= the
  * nParticles it was created with); the next pbf_step captures its graph again

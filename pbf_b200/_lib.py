@@ -59,7 +59,7 @@ class ExtParams(C.Structure):
         ("cell_order", C.c_int), ("flags", C.c_uint), ("scorr_scale", C.c_float),
         ("sphere", C.c_float * 4), ("adaptive", C.c_int), ("density_tol", C.c_float),
         ("max_iterations", C.c_int), ("measure_error", C.c_int), ("debug", C.c_int),
-        ("warm_start", C.c_int), ("profile", C.c_int), ("block_size", C.c_int), ("record_features", C.c_int), ("warm_clamp", C.c_float), ("pair_lanes", C.c_int), ("reserved", C.c_int * 3),
+        ("warm_start", C.c_int), ("profile", C.c_int), ("block_size", C.c_int), ("record_features", C.c_int), ("warm_clamp", C.c_float), ("pair_lanes", C.c_int), ("persistent", C.c_int), ("warm_unfused", C.c_int), ("reserved", C.c_int * 1),
     ]
 
 
@@ -123,6 +123,7 @@ _PROTOS = [
     ("pbf_host_fence", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pbf_debug_fail_staging_alloc", C.c_int, [C.c_int]),
     ("pbf_debug_expire_wait", C.c_int, [C.c_int, C.POINTER(C.c_int)]),
+    ("pbf_measure_fp32_peak", C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("pbf_resize", C.c_int, [C.c_void_p, C.c_int]),
     ("pbf_set_parameter", C.c_int, [C.c_void_p, C.POINTER(SolverParameter)]),
     ("pbf_download_sorted_device", C.c_int, [C.c_void_p] + [C.c_void_p] * 5 + [C.c_void_p]),

@@ -1,7 +1,8 @@
 """Autotuner for the neighbour passes: picks the threads per block, the pair
-lanes per particle and the grid cell size (h or h/2 with a 5x5x5 stencil) of a
-workload by timing each candidate on the GPU from the same initial state, and
-caches the choice.
+lanes per particle, the grid cell size (h or h/2 with a 5x5x5 stencil) and
+whether each pass is one persistent launch (resident blocks striding over all
+tiles of slots) of a workload by timing each candidate on the GPU from the same
+initial state, and caches the choice.
 
 The candidates change the launch shape, the neighbour-list order and the FP32
 summation order (pair lanes), never the neighbour sets (test_gpu_batch.py checks
@@ -15,7 +16,7 @@ import math
 import os
 from typing import Optional, Sequence
 
-CANDIDATES = [(cs, bs, ln) for cs in (1.0, 0.5) for bs in (128, 256) for ln in (1, 2, 4)]
+CANDIDATES = [(cs, bs, ln, ps) for cs in (1.0, 0.5) for bs in (64, 128, 256) for ln in (1, 2, 4) for ps in (0, 1)]
 
 
 def dims_for_scale(dims: Sequence[int], cell_scale: float) -> list:
@@ -30,10 +31,11 @@ def signature(scenes, iterations: int) -> str:
 
 def ext_for(tuned: dict) -> dict:
     """Ext overrides of a tuning result (grid_dims excluded: they are per scene)."""
-    return {"cell_scale": tuned["cell_scale"], "block_size": tuned["block_size"], "pair_lanes": tuned["pair_lanes"]}
+    return {"cell_scale": tuned["cell_scale"], "block_size": tuned["block_size"], "pair_lanes": tuned["pair_lanes"],
+            "persistent": tuned.get("persistent", 0)}
 
 
-def _time_candidate(scenes, iterations, cell_scale, block, lanes, substeps, warm):
+def _time_candidate(scenes, iterations, cell_scale, block, lanes, persistent, substeps, warm):
     import torch
 
     from . import scenes as S
@@ -43,13 +45,14 @@ def _time_candidate(scenes, iterations, cell_scale, block, lanes, substeps, warm
         sc = scs[0]
         dims = dims_for_scale(sc.ext_overrides["grid_dims"], cell_scale)
         s = Solver(sc.para, sc.grid_space, sc.boundary,
-                   sc.ext(grid_dims=dims, cell_scale=cell_scale, block_size=block, pair_lanes=lanes))
+                   sc.ext(grid_dims=dims, cell_scale=cell_scale, block_size=block, pair_lanes=lanes,
+                          persistent=persistent))
         s.upload(sc.pos, sc.vel)
     else:
         para, descs, ov, pos, vel = S.batch_inputs(scs, iterations=iterations)
         for d in descs:
             d["grid_dims"] = dims_for_scale(d["grid_dims"], cell_scale)
-        ov.update(cell_scale=cell_scale, block_size=block, pair_lanes=lanes)
+        ov.update(cell_scale=cell_scale, block_size=block, pair_lanes=lanes, persistent=persistent)
         s = BatchSolver(para, descs, S.default_ext(**ov))
         s.upload(pos, vel)
     st = torch.cuda.current_stream()
@@ -66,8 +69,9 @@ def _time_candidate(scenes, iterations, cell_scale, block, lanes, substeps, warm
 
 def tune(scenes, iterations: int = 4, substeps: int = 6, warm: int = 2, candidates=None,
          cache_path: Optional[str] = None) -> dict:
-    """Times every (cell_scale, block_size, pair_lanes) candidate and returns the
-    fastest: {"cell_scale", "block_size", "pair_lanes", "ms_per_substep", "table"}."""
+    """Times every (cell_scale, block_size, pair_lanes, persistent) candidate and
+    returns the fastest: {"cell_scale", "block_size", "pair_lanes", "persistent",
+    "ms_per_substep", "table"}."""
     key = signature(scenes, iterations)
     if cache_path and os.path.exists(cache_path):
         with open(cache_path) as f:
@@ -75,9 +79,11 @@ def tune(scenes, iterations: int = 4, substeps: int = 6, warm: int = 2, candidat
         if key in cache:
             return cache[key]
     table = []
-    for cs, bs, ln in candidates or CANDIDATES:
-        table.append({"cell_scale": cs, "block_size": bs, "pair_lanes": ln,
-                      "ms_per_substep": _time_candidate(scenes, iterations, cs, bs, ln, substeps, warm)})
+    for cand in candidates or CANDIDATES:
+        cs, bs, ln = cand[:3]
+        ps = cand[3] if len(cand) > 3 else 0
+        table.append({"cell_scale": cs, "block_size": bs, "pair_lanes": ln, "persistent": ps,
+                      "ms_per_substep": _time_candidate(scenes, iterations, cs, bs, ln, ps, substeps, warm)})
     best = min(table, key=lambda r: r["ms_per_substep"])
     out = dict(best)
     out["table"] = table

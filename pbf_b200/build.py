@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpbf_b200.so")
 
 SOURCES = ["pbf_kernels.cu", "pbf_pairs.cu", "pbf_mlp.cu", "pbf_capi.cu", "pbf_noalloc.cu", "pbf_render.cu"]
-HEADERS = ["pbf_device.cuh", "pbf_kernels.h", "pbf_mlp.h", "pbf_tc.cuh", "pbf_packed.cuh"]
+HEADERS = ["pbf_device.cuh", "pbf_kernels.h", "pbf_mlp.h", "pbf_mlp_dev.cuh", "pbf_tc.cuh", "pbf_packed.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-fmad=false", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 

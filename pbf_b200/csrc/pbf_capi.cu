@@ -14,6 +14,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/pbf.h"
 #include "pbf_kernels.h"
 #include "pbf_mlp.h"
@@ -21,6 +23,16 @@
 using namespace pbf;
 
 namespace {
+
+// NVTX range over a scope: every public call that enqueues work is one range,
+// and while a substep graph is captured each phase is a range named after it
+// (header-only NVTX: without a profiler attached a push/pop is a no-op call).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 thread_local std::string g_err;
 
@@ -182,6 +194,7 @@ KParams make_kparams(const pbf_solver& s) {
     k.n = s.n;
     k.block = e.block_size > 0 ? e.block_size : 256;
     k.lanes = e.pair_lanes > 0 ? e.pair_lanes : 2;
+    k.persistent = e.persistent;
     k.max_nbr = e.max_neighbors;
     k.stride = s.stride;
     k.cell_order = e.cell_order;
@@ -297,16 +310,23 @@ int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, co
     if (!std::isfinite(e->warm_clamp) || e->warm_clamp < 0) return fail(PBF_ERR_INVALID, "warm_clamp must be >= 0");
     if (e->pair_lanes != 0 && e->pair_lanes != 1 && e->pair_lanes != 2 && e->pair_lanes != 4 && e->pair_lanes != 8)
         return fail(PBF_ERR_INVALID, "pair_lanes must be 0, 1, 2, 4 or 8");
+    if (e->persistent != 0 && e->persistent != 1) return fail(PBF_ERR_INVALID, "persistent must be 0 or 1");
+    if (e->warm_unfused != 0 && e->warm_unfused != 1) return fail(PBF_ERR_INVALID, "warm_unfused must be 0 or 1");
     return PBF_OK;
 }
 
 // Wraps each launch in a pair of timing events when ext.profile is set; the
 // events are captured into the graph and read back by pbf_stage_times.
+const char* const kStageNames[ST_COUNT] = {"hash", "scan", "scatter", "reorder", "neighbours", "lambda", "dp",
+                                            "velocity", "curl", "vorticity", "copy", "density error",
+                                            "warm-start mlp"};
+
 struct Prof {
     pbf_solver* s;
     cudaStream_t st;
     bool on;
     template <typename F> void operator()(int stage, F&& f) {
+        NvtxRange range(kStageNames[stage]);
         if (!on) {
             f();
             return;
@@ -413,13 +433,25 @@ int enqueue_substep(pbf_solver* s, cudaStream_t st) {
     // (and the 12 features); with a warm start the MLP replaces it by lambda0.
     int first = 0;
     if (feats && iters > 0) {
-        P(ST_LAMBDA, [&] {
-            launch_features(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->lam_prev_sorted, s->Q, s->feat, s->lam_acc, st);
-        });
-        if (warm)
-            P(ST_MLP, [&] {
-                mlp_infer(s->mlp_w, s->mlp_b, s->feat, n, s->lam0, s->Q, s->lam_acc, s->ext.warm_clamp, err, st);
+        if (warm && !s->ext.warm_unfused) {
+            // features, plain lambda and the network in one pass (the features stay
+            // on chip; they reach s->feat only when recorded for training)
+            int rc = 0;
+            P(ST_LAMBDA, [&] {
+                rc = launch_features_warm(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->lam_prev_sorted, s->Q,
+                                          s->ext.record_features ? s->feat : nullptr, s->lam_acc, s->mlp_w, s->mlp_b,
+                                          s->lam0, s->ext.warm_clamp, err, st);
             });
+            if (rc) return fail(PBF_ERR_CUDA, "fused warm-start pass: launch configuration failed");
+        } else {
+            P(ST_LAMBDA, [&] {
+                launch_features(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->lam_prev_sorted, s->Q, s->feat, s->lam_acc, st);
+            });
+            if (warm)
+                P(ST_MLP, [&] {
+                    mlp_infer(s->mlp_w, s->mlp_b, s->feat, n, s->lam0, s->Q, s->lam_acc, s->ext.warm_clamp, err, st);
+                });
+        }
         const bool last = !s->ext.adaptive && iters == 1;
         P(ST_DP, [&] {
             launch_dp(kp, dbg, s->Q, s->nbr, s->ncnt, s->Pxold, s->Px, last ? s->Pv : nullptr, s->dp_dbg, IterCtl{},
@@ -482,6 +514,7 @@ int enqueue_substep(pbf_solver* s, cudaStream_t st) {
 }
 
 int build_graph(pbf_solver* s) {
+    NvtxRange range("capture substep graph");
     if (s->exec) {
         cudaGraphExecDestroy(s->exec);
         s->exec = nullptr;
@@ -739,6 +772,7 @@ int pbf_destroy(pbf_solver* s) {
 }
 
 int pbf_upload_device(pbf_solver* s, const float* d_pos, const float* d_vel, int n, void* stream) {
+    NvtxRange range("pbf_upload_device");
     if (!s || !d_pos || !d_vel) return fail(PBF_ERR_INVALID, "null argument");
     if (n != s->n) return fail(PBF_ERR_INVALID, "n (%d) differs from nParticles (%d)", n, s->n);
     cudaStream_t st = (cudaStream_t)stream;
@@ -758,6 +792,7 @@ int pbf_upload_device(pbf_solver* s, const float* d_pos, const float* d_vel, int
 }
 
 int pbf_upload(pbf_solver* s, const float* pos, const float* vel, int n) {
+    NvtxRange range("pbf_upload");
     if (!s || !pos || !vel) return fail(PBF_ERR_INVALID, "null argument");
     if (n != s->n) return fail(PBF_ERR_INVALID, "n (%d) differs from nParticles (%d)", n, s->n);
     for (size_t i = 0; i < (size_t)3 * n; ++i)
@@ -778,6 +813,7 @@ int pbf_bind_position(pbf_solver* s, float* d_pos) {
 }
 
 int pbf_step(pbf_solver* s, int substeps, void* stream) {
+    NvtxRange range("pbf_step");
     if (!s) return fail(PBF_ERR_INVALID, "null handle");
     if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_step before pbf_upload");
     if (substeps < 0) return fail(PBF_ERR_INVALID, "negative substep count");
@@ -798,6 +834,7 @@ int pbf_step(pbf_solver* s, int substeps, void* stream) {
 }
 
 int pbf_step_host(pbf_solver* s, const float* pos, const float* vel, float* pos_out, int substeps, void* stream) {
+    NvtxRange range("pbf_step_host");
     if (!s || !pos || !vel || !pos_out) return fail(PBF_ERR_INVALID, "null argument");
     if (substeps < 0) return fail(PBF_ERR_INVALID, "negative substep count");
     if (!s->hp) {
@@ -888,6 +925,13 @@ int pbf_debug_expire_wait(int which, int* error_bits) {
     return PBF_OK;
 }
 
+int pbf_measure_fp32_peak(double* scalar_tflops, double* packed_tflops) {
+    if (!scalar_tflops || !packed_tflops) return fail(PBF_ERR_INVALID, "null argument");
+    NvtxRange range("pbf_measure_fp32_peak");
+    if (measure_fp32_peak(scalar_tflops, packed_tflops)) return fail(PBF_ERR_CUDA, "FP32 throughput probe failed");
+    return PBF_OK;
+}
+
 int pbf_debug_fail_staging_alloc(int k) {
     if (k < 0) return fail(PBF_ERR_INVALID, "k must be >= 0");
     g_fail_staging_alloc.store(k);
@@ -957,6 +1001,7 @@ int pbf_download_sorted_device(pbf_solver* s, float* d_pos, float* d_vel, int* d
 }
 
 int pbf_build_grid(pbf_solver* s, void* stream) {
+    NvtxRange range("pbf_build_grid");
     if (!s) return fail(PBF_ERR_INVALID, "null handle");
     if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_build_grid before pbf_upload");
     cudaStream_t st = (cudaStream_t)stream;
@@ -983,6 +1028,7 @@ int pbf_build_grid(pbf_solver* s, void* stream) {
 }
 
 int pbf_download_device(pbf_solver* s, float* d_pos, float* d_vel, void* stream) {
+    NvtxRange range("pbf_download_device");
     if (!s) return fail(PBF_ERR_INVALID, "null handle");
     if (!s->uploaded) return fail(PBF_ERR_STATE, "pbf_download before pbf_upload");
     cudaStream_t st = (cudaStream_t)stream;

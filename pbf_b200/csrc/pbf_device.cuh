@@ -75,6 +75,7 @@ struct KParams {
     int stride;     // neighbour list stride (slot-major layout: nbr[q * stride + k])
     int cell_order; // 0 ascending, 1 descending within a cell
     int n_int;      // s_corr exponent when a small integer, else 0
+    int persistent; // neighbour passes: resident blocks striding over the tiles of slots
     unsigned flags;
     double poly6_c64;  // exact poly6 constant for the FP64 density reduction
     // wall density: n_wall (rest number density), 1/h, 315/(256 h), Horner coefficients

@@ -14,6 +14,8 @@
 // calculateParticlesGid :31-40, calculatePrefixSum :42-89, addBlockSum :91-96,
 // setGrid :99-111, countingSort :112-122, buildNeighborhood :124-154; the
 // neighbour-sum passes (lambda, dp, curl, vorticity) are in pbf_pairs.cu.
+#include <algorithm>
+
 #include "pbf_kernels.h"
 #include "pbf_packed.cuh"
 
@@ -347,10 +349,9 @@ __global__ void __launch_bounds__(256, 8) k_reorder(KParams p, const float4* __r
 // thread waits on a few independent loads at once instead of one chain per row
 // and per candidate.
 template <int RR>
-__global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __restrict__ x,
-                                                   const int* __restrict__ cell_start, int* __restrict__ nbr,
-                                                   int* __restrict__ ncnt) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void neighbors_one(const KParams& p, int k, const float4* __restrict__ x,
+                                              const int* __restrict__ cell_start, int* __restrict__ nbr,
+                                              int* __restrict__ ncnt) {
     if (k >= p.n) return;
     const SceneView sc = scene_of(p, k);
     const f3 xk = make3(x[k]);
@@ -456,6 +457,16 @@ __global__ void __launch_bounds__(256) k_neighbors(KParams p, const float4* __re
         }
     }
     ncnt[k] = c;
+}
+
+// nvb tiles of blockDim.x slots; the grid strides over them (a grid of nvb
+// blocks is the ordinary one-block-per-tile launch)
+template <int RR>
+__global__ void __launch_bounds__(256) k_neighbors(KParams p, int nvb, const float4* __restrict__ x,
+                                                   const int* __restrict__ cell_start, int* __restrict__ nbr,
+                                                   int* __restrict__ ncnt) {
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x)
+        neighbors_one<RR>(p, vb * blockDim.x + threadIdx.x, x, cell_start, nbr, ncnt);
 }
 
 // Copies features and total lambda of the given slots (training rows).
@@ -615,6 +626,79 @@ __global__ void k_copy4(int n, const float4* __restrict__ a, float4* __restrict_
 }
 
 // ---------------------------------------------------------------------------
+// FP32 throughput probe: every thread runs 8 independent chains of fused
+// multiply-adds (scalar FFMA, or packed fma.rn.f32x2 with two lanes each), long
+// enough that launch and tail are negligible. The result is stored only under a
+// condition the chains never meet, so nothing is optimised away and nothing is
+// written. FLOPs = 2 per multiply-add lane.
+// ---------------------------------------------------------------------------
+template <bool PACKED>
+__global__ void __launch_bounds__(256) k_fma_peak(int iters, float seed, float* __restrict__ sink) {
+    const float b = 0.999999f, c = 1e-7f;
+    if (PACKED) {
+        float2 a[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a[i] = make_float2(seed + (float)(threadIdx.x + i), seed - (float)i);
+        for (int it = 0; it < iters; ++it) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = vfma(a[i], bc<float2>(b), bc<float2>(c));
+        }
+        float t = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) t += a[i].x + a[i].y;
+        if (t == -1.0f) sink[threadIdx.x] = t;
+    } else {
+        float a[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a[i] = seed + (float)(threadIdx.x + i);
+        for (int it = 0; it < iters; ++it) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = __fmaf_rn(a[i], b, c);
+        }
+        float t = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) t += a[i];
+        if (t == -1.0f) sink[threadIdx.x] = t;
+    }
+}
+
+// Best of three timed launches of each form (CUDA events), after a warm-up launch.
+int measure_fp32_peak(double* scalar_tflops, double* packed_tflops) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    float* sink = nullptr;
+    if (cudaMalloc(&sink, 256 * sizeof(float)) != cudaSuccess) return -1;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    double best[2] = {0.0, 0.0};
+    for (int form = 0; form < 2; ++form) {
+        const double lanes = form ? 2.0 : 1.0;
+        const double flops = 2.0 * 8.0 * lanes * iters * (double)blocks * threads;
+        for (int rep = 0; rep < 4; ++rep) {
+            cudaEventRecord(a, 0);
+            if (form) k_fma_peak<true><<<blocks, threads>>>(iters, 1.0f, sink);
+            else k_fma_peak<false><<<blocks, threads>>>(iters, 1.0f, sink);
+            cudaEventRecord(b, 0);
+            cudaEventSynchronize(b);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (rep > 0 && ms > 0.0f) best[form] = std::max(best[form], flops / (ms * 1e-3) / 1e12);
+        }
+    }
+    const cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return -1;
+    *scalar_tflops = best[0];
+    *packed_tflops = best[1];
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 static inline int blocks_for(int n, int bs) { return (n + bs - 1) / bs; }
@@ -697,11 +781,24 @@ void launch_reorder(const KParams& p, bool predict_on, const float4* x, const fl
                                             lam_in, lam_out, err);
 }
 
+// Grid over nvb tiles: nvb blocks, or with p.persistent the blocks resident at
+// once (SMs x blocks per SM), each striding over the tiles.
+template <typename K> static int resident_grid(const KParams& p, K kernel, int nvb) {
+    if (!p.persistent) return nvb;
+    int dev = 0, sms = 1, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, p.block, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 1;
+    const long long g = (long long)per_sm * (sms > 0 ? sms : 1);
+    return (int)(g < nvb ? g : nvb);
+}
+
 void launch_neighbors(const KParams& p, const float4* x, const int* cell_start, int* nbr, int* ncnt, cudaStream_t st) {
     const int b = blocks_for(p.n, p.block);
-    if (p.radius == 1) k_neighbors<1><<<b, p.block, 0, st>>>(p, x, cell_start, nbr, ncnt);
-    else if (p.radius == 2) k_neighbors<2><<<b, p.block, 0, st>>>(p, x, cell_start, nbr, ncnt);
-    else k_neighbors<0><<<b, p.block, 0, st>>>(p, x, cell_start, nbr, ncnt);
+    if (p.radius == 1) k_neighbors<1><<<resident_grid(p, k_neighbors<1>, b), p.block, 0, st>>>(p, b, x, cell_start, nbr, ncnt);
+    else if (p.radius == 2) k_neighbors<2><<<resident_grid(p, k_neighbors<2>, b), p.block, 0, st>>>(p, b, x, cell_start, nbr, ncnt);
+    else k_neighbors<0><<<resident_grid(p, k_neighbors<0>, b), p.block, 0, st>>>(p, b, x, cell_start, nbr, ncnt);
 }
 
 void launch_gather_rows(const int* slots, int count, int n, const float* feat, const float* lam_acc, float* out_feat,

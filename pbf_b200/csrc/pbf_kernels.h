@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
+#include <stdint.h>
 
 #include "pbf_device.cuh"
 
@@ -33,6 +34,12 @@ void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, c
                float4* xout, float4* vout, float4* dp, const IterCtl& ctl, cudaStream_t st);
 void launch_features(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
                      const float* lam_prev, float4* xl, float* feat, float* lam_acc, cudaStream_t st);
+// The first lambda pass of a warm-started substep fused with the network on the
+// tensor cores: writes xl = (x, lambda0), lam_acc = lam0 = lambda0 (feat only
+// when not null). Returns nonzero when the launch could not be configured.
+int launch_features_warm(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
+                         const float* lam_prev, float4* xl, float* feat, float* lam_acc, const uint16_t* w,
+                         const float* b, float* lam0, float clamp, int* err, cudaStream_t st);
 void launch_gather_rows(const int* slots, int count, int n, const float* feat, const float* lam_acc, float* out_feat,
                         float* out_target, int* err, cudaStream_t st);
 void launch_count_fallback(const int* iters, int first, int configured, int* fallback, long long* total,
@@ -59,6 +66,10 @@ void launch_copy4(int n, const float4* a, float4* b, cudaStream_t st);
 void launch_sorted_state(int n, const float4* x, const float4* v, const int* perm, const int* cell_sorted,
                          const int* cell_start, float* pos, float* vel, int* ids, int* key, int* rank,
                          cudaStream_t st);
+
+// FP32 fused multiply-add throughput of the current device, scalar and packed
+// (f32x2), in TFLOP/s; synchronises the device. 0 on success.
+int measure_fp32_peak(double* scalar_tflops, double* packed_tflops);
 
 // Records the message returned by pbf_last_error() for this thread; returns code.
 int set_last_error(int code, const char* msg);

@@ -23,8 +23,11 @@
 // every sum, which leaves the sum unchanged: no accumulator is ever -0 (they
 // start at +0, and in round-to-nearest x + (-x) = +0 and +0 + (-0) = +0).
 #include "pbf_kernels.h"
+#include "pbf_mlp.h"
+#include "pbf_mlp_dev.cuh"
 #include "pbf_packed.cuh"
 
+#include <algorithm>
 #include <type_traits>
 
 namespace pbf {
@@ -150,10 +153,12 @@ template <int L> struct Team {
     unsigned mask;  // the team's lanes within the warp
 };
 
-// blockDim.x is a multiple of 32, so a team never straddles a warp
-template <int L> __device__ __forceinline__ Team<L> team_of() {
+// blockDim.x is a multiple of 32, so a team never straddles a warp. vb is the
+// virtual block: blockIdx.x for one block per tile of slots, or one of the tiles
+// a persistent block strides over.
+template <int L> __device__ __forceinline__ Team<L> team_of(int vb) {
     Team<L> m;
-    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long g = (long long)vb * blockDim.x + threadIdx.x;
     m.k = (int)(g / L);
     m.t = (int)(threadIdx.x & (L - 1));
     const int lane = threadIdx.x & 31;
@@ -212,6 +217,7 @@ __device__ __forceinline__ void block_error_reduce(float e, unsigned long long* 
         atomicMax(max_bits, (unsigned long long)__double_as_longlong((double)m));
         atomicAdd(sum, dsum);
     }
+    __syncthreads();  // a persistent block's next tile writes s_max / s_sum again
 }
 
 // Neighbour entries per thread and batch: four in every pass (V entries per
@@ -223,13 +229,12 @@ template <int V> __host__ __device__ constexpr int batches() { return 4 / V; }
 // one-sided density error of the positions it sees
 // ---------------------------------------------------------------------------
 template <bool DEBUG, int L, int V>
-__global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_lambda(KParams p, const float4* __restrict__ x, const int* __restrict__ nbr,
-                                                const int* __restrict__ ncnt, float4* __restrict__ xl,
-                                                float* __restrict__ rho_out, IterCtl ctl) {
+__device__ __forceinline__ void lambda_tile(const KParams& p, int vb, const float4* __restrict__ x,
+                                            const int* __restrict__ nbr, const int* __restrict__ ncnt,
+                                            float4* __restrict__ xl, float* __restrict__ rho_out, const IterCtl& ctl) {
     using T = vec_t<V>;
     constexpr int P = L * V, B = batches<V>();
-    if (ctl.done && *ctl.done) return;
-    const Team<L> tm = team_of<L>();
+    const Team<L> tm = team_of<L>(vb);
     const int k = tm.k;
     float err = 0.0f;
     if (k < p.n) {
@@ -290,6 +295,17 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_lambda(KParams p, const
     }
 }
 
+// nvb tiles of blockDim.x slots' teams; the grid strides over them (a grid of
+// nvb blocks is the ordinary one-block-per-tile launch)
+template <bool DEBUG, int L, int V>
+__global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_lambda(KParams p, int nvb, const float4* __restrict__ x,
+                                                                const int* __restrict__ nbr,
+                                                                const int* __restrict__ ncnt, float4* __restrict__ xl,
+                                                                float* __restrict__ rho_out, IterCtl ctl) {
+    if (ctl.done && *ctl.done) return;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) lambda_tile<DEBUG, L, V>(p, vb, x, nbr, ncnt, xl, rho_out, ctl);
+}
+
 // ---------------------------------------------------------------------------
 // a17: warm-start features (no reference counterpart), computed in the first
 // lambda pass of a substep together with that pass's lambda (the same
@@ -306,17 +322,19 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_lambda(KParams p, const
 // None depends on the grid's cell size. lam_acc starts the substep's total lambda
 // at this pass's lambda.
 // ---------------------------------------------------------------------------
+// One team's particle: writes xl[k] = (x, plain lambda), lam_acc[k] = lambda
+// and, when feat is not null, the 12 features; returns true on the team's first
+// thread (with the features in f and the plain lambda in lam) when k < n.
 template <int L, int V>
-__global__ void __launch_bounds__(256) k_features(KParams p, const float4* __restrict__ x,
-                                                  const float4* __restrict__ v, const int* __restrict__ nbr,
-                                                  const int* __restrict__ ncnt, const float* __restrict__ lam_prev,
-                                                  float4* __restrict__ xl, float* __restrict__ feat,
-                                                  float* __restrict__ lam_acc) {
+__device__ __forceinline__ bool features_one(const KParams& p, const Team<L>& tm, const float4* __restrict__ x,
+                                             const float4* __restrict__ v, const int* __restrict__ nbr,
+                                             const int* __restrict__ ncnt, const float* __restrict__ lam_prev,
+                                             float4* __restrict__ xl, float* __restrict__ feat,
+                                             float* __restrict__ lam_acc, float (&f)[12], float& lam) {
     using T = vec_t<V>;
     constexpr int P = L * V, B = batches<V>();
-    const Team<L> tm = team_of<L>();
     const int k = tm.k;
-    if (k >= p.n) return;  // uniform over the team
+    if (k >= p.n) return false;  // uniform over the team
     const f3 xk = make3(x[k]);
     const f3 vk = make3(v[k]);
     const int cnt = ncnt[k];
@@ -367,7 +385,7 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
     const float closes = team_sum<L>(fold(close), tm.mask);
     const f3 r3 = team_sum3<L>(fold3(rs), tm.mask);
     const float dv2s = team_sum<L>(fold(dv2), tm.mask);
-    if (tm.t != 0) return;
+    if (tm.t != 0) return false;
     const SceneView sc = scene_of(p, k);
     const float rho_fluid = rhos;
     const float gsl = __fsqrt_rn(dot_fma(g3, g3));
@@ -382,12 +400,11 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
     gms = __fmaf_rn(g3.y, g3.y, gms);
     gms = __fmaf_rn(g3.z, g3.z, gms);
     gms = __fdiv_rn(gms, p.rho0sq);
-    const float lam = __fdiv_rn(-C, gms + p.eps);
+    lam = __fdiv_rn(-C, gms + p.eps);
     xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
     lam_acc[k] = lam;
 
     const float inv_cnt = 1.0f / (float)max(cnt, 1);
-    float f[12];
     f[0] = (float)cnt / (float)p.max_nbr;
     f[1] = rho_fluid / p.rho0;
     f[2] = lam_prev[k];
@@ -404,8 +421,175 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
     f[10] = gsl * p.h / p.rho0;
     const float dth = p.dt * p.inv_h;
     f[11] = dv2s * (dth * dth) * inv_cnt;
+    if (feat) {
 #pragma unroll
-    for (int i = 0; i < 12; ++i) feat[(size_t)k * 12 + i] = f[i];
+        for (int i = 0; i < 12; ++i) feat[(size_t)k * 12 + i] = f[i];
+    }
+    return true;
+}
+
+template <int L, int V>
+__global__ void __launch_bounds__(256) k_features(KParams p, int nvb, const float4* __restrict__ x,
+                                                  const float4* __restrict__ v, const int* __restrict__ nbr,
+                                                  const int* __restrict__ ncnt, const float* __restrict__ lam_prev,
+                                                  float4* __restrict__ xl, float* __restrict__ feat,
+                                                  float* __restrict__ lam_acc) {
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        float f[12], lam;
+        features_one<L, V>(p, team_of<L>(vb), x, v, nbr, ncnt, lam_prev, xl, feat, lam_acc, f, lam);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// a17, fused: the first lambda pass of a warm-started substep with the network
+// in the same kernel. Each block computes its particles' features and plain
+// lambda as k_features does; the team leaders write their normalised features
+// as BF16 straight into the tensor core's A tile in shared memory (K-major,
+// never to HBM), and the block evaluates 12 -> 64 -> 64 -> 64 on the tensor
+// cores (one 128-row MMA per tile of rows and layer, issued by one thread,
+// accumulated in TMEM, 64 columns per tile) with the GELU epilogues on the CUDA
+// cores, then the output layer and the trust region. Thread t runs the
+// epilogue of row t: a warp reads its quarter of the TMEM lanes, and the warps
+// of the second half of a 256-thread block the second tile's columns. While
+// one block waits on its MMAs the SM runs the other resident blocks' gathers.
+// The arithmetic is k_mlp_fwd's (same operands, MMA shapes and epilogue), so
+// lambda0 is the unfused path's bit for bit.
+// ---------------------------------------------------------------------------
+struct WarmIO {
+    const uint16_t* w;  // BF16 weights (W1 [64][16], W2, W3 [64][64], w4 [64])
+    const float* b;     // biases and constants (normalisation, output scale)
+    float* lam0;        // lambda0 per slot
+    float clamp;        // trust region around the plain lambda (0: none)
+    int* err;           // PBF_DEVERR_MLP_TIMEOUT on an expired tensor-core wait
+};
+
+constexpr int FW_SW1 = 0;                     // W1 [64 x 16]  2 KB
+constexpr int FW_SW2 = FW_SW1 + 64 * 16 * 2;  // W2 [64 x 64]  8 KB
+constexpr int FW_SW3 = FW_SW2 + 64 * 64 * 2;  // W3 [64 x 64]  8 KB
+constexpr int FW_SX = FW_SW3 + 64 * 64 * 2;   // X: per tile [128 x 16] BF16, 4 KB; then H: per tile [128 x 64], 16 KB
+constexpr int FW_X_TILE = 128 * 16 * 2;
+constexpr int FW_H_TILE = 128 * 64 * 2;
+__host__ __device__ constexpr int warm_smem_bytes(int tiles) { return FW_SX + tiles * (FW_X_TILE + FW_H_TILE); }
+
+template <int L, int V>
+__global__ void __launch_bounds__(256, 3) k_features_warm(KParams p, int nvb, const float4* __restrict__ x,
+                                                          const float4* __restrict__ v, const int* __restrict__ nbr,
+                                                          const int* __restrict__ ncnt,
+                                                          const float* __restrict__ lam_prev,
+                                                          float4* __restrict__ xl, float* __restrict__ feat,
+                                                          float* __restrict__ lam_acc, WarmIO io) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ float sb[MLP_NUM_BIASES];
+    __shared__ float sw4[64];
+    __shared__ float s_lam[256];
+    const int t = threadIdx.x, warp = t >> 5;
+    const int R = blockDim.x / L;            // particles per tile of slots: rows
+    const int tiles = (R + 127) >> 7;        // 128-row MMA tiles
+    const uint32_t cols = tiles > 1 ? 128u : 64u;
+    uint8_t* sX = smem + FW_SX;
+    uint8_t* sH = sX + tiles * FW_X_TILE;
+    if (warp == 0) tmem_alloc(&tmem_slot, cols);
+    if (t == 0) mbar_init(&mbar, 1);
+    stage_weight(smem + FW_SW1, io.w + W1_OFF, 64, 16);
+    stage_weight(smem + FW_SW2, io.w + W2_OFF, 64, 64);
+    stage_weight(smem + FW_SW3, io.w + W3_OFF, 64, 64);
+    for (int i = t; i < MLP_NUM_BIASES; i += blockDim.x) sb[i] = io.b[i];
+    if (t < 64) sw4[t] = bf16_val(io.w[W4_OFF + t]);
+    // rows of the last tile past R stay zero
+    for (int i = t; i < tiles * FW_X_TILE / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(sX)[i] = make_uint4(0u, 0u, 0u, 0u);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tbase = tmem_slot;
+    const bool ep_warp = (warp >> 2) < tiles;  // this warp's TMEM quarter holds rows of a tile
+    const uint32_t lane_base = tmem_addr(tbase, 32 * (warp & 3), 64 * (warp >> 2));
+    uint8_t* my_h = sH + (warp >> 2) * FW_H_TILE;
+    uint32_t phase = 0;
+    bool alive = true;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        const Team<L> tm = team_of<L>(vb);
+        float f[12], lam = 0.0f;
+        const bool have = features_one<L, V>(p, tm, x, v, nbr, ncnt, lam_prev, xl, feat, lam_acc, f, lam);
+        if (tm.t == 0) {
+            const int row = t / L;
+            float xf[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) xf[i] = 0.0f;
+            if (have) {
+#pragma unroll
+                for (int i = 0; i < MLP_IN; ++i) xf[i] = (f[i] - sb[FMEAN_OFF + i]) * sb[FISTD_OFF + i];
+            }
+            uint32_t pk[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                pk[i] = (uint32_t)bf16_bits(xf[2 * i]) | ((uint32_t)bf16_bits(xf[2 * i + 1]) << 16);
+            uint8_t* xt = sX + (row >> 7) * FW_X_TILE;
+            *reinterpret_cast<uint4*>(xt + kmajor_offset(row & 127, 0, 128)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            *reinterpret_cast<uint4*>(xt + kmajor_offset(row & 127, 8, 128)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            s_lam[row] = lam;
+        }
+        if (!alive) continue;  // an expired wait: no more tensor-core work (the error bit is set)
+        // three hidden layers; layer l reads X (l = 0) or H and writes H (l < 2)
+        float y = sb[B4_OFF];
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            sync_for_mma();
+            if (t == 0) {
+                for (int j = 0; j < tiles; ++j) {
+                    if (l == 0) gemm_issue(tbase + 64 * j, sX + j * FW_X_TILE, smem + FW_SW1, 64, 16, 0);
+                    else gemm_issue(tbase + 64 * j, sH + j * FW_H_TILE, smem + (l == 1 ? FW_SW2 : FW_SW3), 64, 64, 0);
+                }
+                commit(&mbar);
+            }
+            if (!wait_mma(&mbar, phase, io.err)) {
+                alive = false;
+                break;
+            }
+            if (ep_warp) {
+                const float* bias = sb + (l == 0 ? B1_OFF : l == 1 ? B2_OFF : B3_OFF);
+#pragma unroll 1
+                for (int c = 0; c < 4; ++c) {
+                    float vv[16];
+                    tmem_ld16(lane_base + 16 * c, vv);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int i = 0; i < 16; i += 2) {
+                        const float2 hh =
+                            gelu2(vadd(make_float2(vv[i], vv[i + 1]),
+                                       make_float2(bias[16 * c + i], bias[16 * c + i + 1])));
+                        vv[i] = hh.x;
+                        vv[i + 1] = hh.y;
+                    }
+                    if (l < 2) {
+                        put_row64(my_h, t & 127, vv, 16 * c);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) y = __fmaf_rn(vv[i], sw4[16 * c + i], y);
+                    }
+                }
+            }
+        }
+        if (!alive) continue;
+        const int k = vb * R + t;
+        if (t < R && k < p.n) {
+            float l0 = y * sb[OSCALE_OFF];
+            if (io.clamp > 0.0f) {
+                // trust region around the plain lambda of this pass: same sign,
+                // at most clamp times its magnitude
+                const float a = io.clamp * s_lam[t];
+                l0 = fminf(fmaxf(l0, fminf(a, 0.0f)), fmaxf(a, 0.0f));
+            }
+            reinterpret_cast<float*>(xl)[4 * (size_t)k + 3] = l0;
+            lam_acc[k] = l0;
+            io.lam0[k] = l0;
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tbase, cols);
 }
 
 // ---------------------------------------------------------------------------
@@ -414,12 +598,17 @@ __global__ void __launch_bounds__(256) k_features(KParams p, const float4* __res
 // (calculateOffset cu:182-199, updatePosition cu:15-22)
 // ---------------------------------------------------------------------------
 template <bool DEBUG, int L, int V>
-__global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_dp(KParams p, const float4* __restrict__ xl, const int* __restrict__ nbr,
-                                            const int* __restrict__ ncnt, const float4* __restrict__ xold,
-                                            float4* __restrict__ xout, float4* __restrict__ vout,
-                                            float4* __restrict__ dp_out, IterCtl ctl) {
-    using T = vec_t<V>;
-    constexpr int P = L * V, B = batches<V>();
+__device__ __forceinline__ void dp_tile(const KParams& p, int vb, const float4* __restrict__ xl,
+                                        const int* __restrict__ nbr, const int* __restrict__ ncnt,
+                                        const float4* __restrict__ xold, float4* __restrict__ xout,
+                                        float4* __restrict__ vout, float4* __restrict__ dp_out);
+
+template <bool DEBUG, int L, int V>
+__global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_dp(KParams p, int nvb, const float4* __restrict__ xl,
+                                                            const int* __restrict__ nbr, const int* __restrict__ ncnt,
+                                                            const float4* __restrict__ xold, float4* __restrict__ xout,
+                                                            float4* __restrict__ vout, float4* __restrict__ dp_out,
+                                                            IterCtl ctl) {
     if (ctl.done) {
         if (*ctl.done) return;
         // the lambda pass just measured the positions this pass would correct;
@@ -434,7 +623,18 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_dp(KParams p, const flo
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(ctl.iters, 1);
     }
-    const Team<L> tm = team_of<L>();
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x)
+        dp_tile<DEBUG, L, V>(p, vb, xl, nbr, ncnt, xold, xout, vout, dp_out);
+}
+
+template <bool DEBUG, int L, int V>
+__device__ __forceinline__ void dp_tile(const KParams& p, int vb, const float4* __restrict__ xl,
+                                        const int* __restrict__ nbr, const int* __restrict__ ncnt,
+                                        const float4* __restrict__ xold, float4* __restrict__ xout,
+                                        float4* __restrict__ vout, float4* __restrict__ dp_out) {
+    using T = vec_t<V>;
+    constexpr int P = L * V, B = batches<V>();
+    const Team<L> tm = team_of<L>(vb);
     const int k = tm.k;
     if (k >= p.n) return;  // uniform over the team
     const float4 xk4 = xl[k];
@@ -493,12 +693,13 @@ __global__ void __launch_bounds__(256, V == 1 ? 6 : 4) k_dp(KParams p, const flo
 // float4s per neighbour (x_j and v_j with |w_j|) instead of three
 // ---------------------------------------------------------------------------
 template <int L, int V>
-__global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restrict__ x, const float4* __restrict__ v,
-                                              const int* __restrict__ nbr, const int* __restrict__ ncnt,
-                                              float4* __restrict__ omega, float4* __restrict__ vw) {
+__device__ __forceinline__ void curl_tile(const KParams& p, int vb, const float4* __restrict__ x,
+                                          const float4* __restrict__ v, const int* __restrict__ nbr,
+                                          const int* __restrict__ ncnt, float4* __restrict__ omega,
+                                          float4* __restrict__ vw) {
     using T = vec_t<V>;
     constexpr int P = L * V, B = batches<V>();
-    const Team<L> tm = team_of<L>();
+    const Team<L> tm = team_of<L>(vb);
     const int k = tm.k;
     if (k >= p.n) return;  // uniform over the team
     const f3 xk = make3(x[k]);
@@ -536,6 +737,14 @@ __global__ void __launch_bounds__(256) k_curl(KParams p, const float4* __restric
         omega[k] = make_float4(w3.x, w3.y, w3.z, wl);
         vw[k] = make_float4(vk.x, vk.y, vk.z, wl);
     }
+}
+
+template <int L, int V>
+__global__ void __launch_bounds__(256) k_curl(KParams p, int nvb, const float4* __restrict__ x,
+                                              const float4* __restrict__ v, const int* __restrict__ nbr,
+                                              const int* __restrict__ ncnt, float4* __restrict__ omega,
+                                              float4* __restrict__ vw) {
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) curl_tile<L, V>(p, vb, x, v, nbr, ncnt, omega, vw);
 }
 
 // ---------------------------------------------------------------------------
@@ -616,24 +825,27 @@ __device__ __forceinline__ int vort_one(const KParams& p, const Team<L>& tm, int
 }
 
 template <bool DEBUG, int L, int V>
-__global__ void __launch_bounds__(256, 4) k_vort(KParams p, const float4* __restrict__ x, const float4* __restrict__ vw,
-                                              const float4* __restrict__ omega, const int* __restrict__ nbr,
-                                              const int* __restrict__ ncnt, float4* __restrict__ xout,
-                                              float4* __restrict__ vout, const int* __restrict__ perm_in,
-                                              int* __restrict__ perm_out, float4* __restrict__ vort_out,
-                                              float4* __restrict__ visc_out, int* __restrict__ cell,
-                                              int* __restrict__ ticket, int* __restrict__ hist, int* __restrict__ err) {
-    const Team<L> tm = team_of<L>();
-    const int k = tm.k;
-    int key = -1;
-    if (k < p.n)  // uniform over the team
-        key = vort_one<DEBUG, L, V>(p, tm, k, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort_out,
-                                    visc_out, err);
-    // the next substep's histogram (every lane of the warp takes part)
-    const int tk = warp_histogram(key, hist);
-    if (key >= 0) {
-        cell[k] = key;
-        ticket[k] = tk;
+__global__ void __launch_bounds__(256, 4) k_vort(KParams p, int nvb, const float4* __restrict__ x,
+                                              const float4* __restrict__ vw, const float4* __restrict__ omega,
+                                              const int* __restrict__ nbr, const int* __restrict__ ncnt,
+                                              float4* __restrict__ xout, float4* __restrict__ vout,
+                                              const int* __restrict__ perm_in, int* __restrict__ perm_out,
+                                              float4* __restrict__ vort_out, float4* __restrict__ visc_out,
+                                              int* __restrict__ cell, int* __restrict__ ticket, int* __restrict__ hist,
+                                              int* __restrict__ err) {
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        const Team<L> tm = team_of<L>(vb);
+        const int k = tm.k;
+        int key = -1;
+        if (k < p.n)  // uniform over the team
+            key = vort_one<DEBUG, L, V>(p, tm, k, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort_out,
+                                        visc_out, err);
+        // the next substep's histogram (every lane of the warp takes part)
+        const int tk = warp_histogram(key, hist);
+        if (key >= 0) {
+            cell[k] = key;
+            ticket[k] = tk;
+        }
     }
 }
 
@@ -642,6 +854,25 @@ __global__ void __launch_bounds__(256, 4) k_vort(KParams p, const float4* __rest
 // ---------------------------------------------------------------------------
 // blocks for n particles with L threads each
 static inline int team_blocks(int n, int L, int bs) { return (int)(((long long)n * L + bs - 1) / bs); }
+
+// Grid of a neighbour pass over nvb tiles: nvb blocks, or with p.persistent the
+// blocks that are resident at once (SMs x blocks per SM at this block size), each
+// striding over the tiles.
+template <typename K> static int pass_grid(const KParams& p, K kernel, int nvb) {
+    if (!p.persistent) return nvb;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, p.block, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 1;
+    const long long g = (long long)per_sm * sms;
+    return (int)(g < nvb ? g : nvb);
+}
 
 // Calls f with (L, V) of pair_lanes as compile-time constants.
 template <int A, int B> struct LV {
@@ -661,8 +892,8 @@ void launch_lambda(const KParams& p, bool debug, const float4* x, const int* nbr
     with_lanes(p.lanes, [&](auto c) {
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
         const int b = team_blocks(p.n, L, p.block);
-        if (debug) k_lambda<true, L, V><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
-        else k_lambda<false, L, V><<<b, p.block, 0, st>>>(p, x, nbr, ncnt, xl, rho, ctl);
+        if (debug) k_lambda<true, L, V><<<pass_grid(p, k_lambda<true, L, V>, b), p.block, 0, st>>>(p, b, x, nbr, ncnt, xl, rho, ctl);
+        else k_lambda<false, L, V><<<pass_grid(p, k_lambda<false, L, V>, b), p.block, 0, st>>>(p, b, x, nbr, ncnt, xl, rho, ctl);
     });
 }
 
@@ -671,8 +902,12 @@ void launch_dp(const KParams& p, bool debug, const float4* xl, const int* nbr, c
     with_lanes(p.lanes, [&](auto c) {
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
         const int b = team_blocks(p.n, L, p.block);
-        if (debug) k_dp<true, L, V><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
-        else k_dp<false, L, V><<<b, p.block, 0, st>>>(p, xl, nbr, ncnt, xold, xout, vout, dp, ctl);
+        if (debug)
+            k_dp<true, L, V><<<pass_grid(p, k_dp<true, L, V>, b), p.block, 0, st>>>(p, b, xl, nbr, ncnt, xold, xout,
+                                                                                     vout, dp, ctl);
+        else
+            k_dp<false, L, V><<<pass_grid(p, k_dp<false, L, V>, b), p.block, 0, st>>>(p, b, xl, nbr, ncnt, xold, xout,
+                                                                                       vout, dp, ctl);
     });
 }
 
@@ -680,16 +915,48 @@ void launch_features(const KParams& p, const float4* x, const float4* v, const i
                      const float* lam_prev, float4* xl, float* feat, float* lam_acc, cudaStream_t st) {
     with_lanes(p.lanes, [&](auto c) {
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
-        k_features<L, V><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, lam_prev, xl, feat,
-                                                                            lam_acc);
+        const int b = team_blocks(p.n, L, p.block);
+        k_features<L, V><<<pass_grid(p, k_features<L, V>, b), p.block, 0, st>>>(p, b, x, v, nbr, ncnt, lam_prev, xl,
+                                                                                 feat, lam_acc);
     });
+}
+
+int launch_features_warm(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
+                         const float* lam_prev, float4* xl, float* feat, float* lam_acc, const uint16_t* w,
+                         const float* b, float* lam0, float clamp, int* err, cudaStream_t st) {
+    int rc = 0;
+    with_lanes(p.lanes, [&](auto c) {
+        constexpr int L = decltype(c)::L, V = decltype(c)::V;
+        const int rows = p.block / L;
+        const int smem = warm_smem_bytes((rows + 127) / 128);
+        if (cudaFuncSetAttribute(k_features_warm<L, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess) {
+            rc = -1;
+            return;
+        }
+        const int nvb = team_blocks(p.n, L, p.block);
+        int grid = nvb;
+        if (p.persistent) {
+            int dev = 0, sms = 1, per_sm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_features_warm<L, V>, p.block, smem) !=
+                    cudaSuccess || per_sm <= 0)
+                per_sm = 1;
+            grid = (int)std::min<long long>((long long)per_sm * sms, nvb);
+        }
+        const WarmIO io{w, b, lam0, clamp, err};
+        k_features_warm<L, V><<<grid, p.block, smem, st>>>(p, nvb, x, v, nbr, ncnt, lam_prev, xl, feat, lam_acc, io);
+    });
+    return rc;
 }
 
 void launch_curl(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt, float4* omega,
                  float4* vw, cudaStream_t st) {
     with_lanes(p.lanes, [&](auto c) {
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
-        k_curl<L, V><<<team_blocks(p.n, L, p.block), p.block, 0, st>>>(p, x, v, nbr, ncnt, omega, vw);
+        const int b = team_blocks(p.n, L, p.block);
+        k_curl<L, V><<<pass_grid(p, k_curl<L, V>, b), p.block, 0, st>>>(p, b, x, v, nbr, ncnt, omega, vw);
     });
 }
 
@@ -700,11 +967,11 @@ void launch_vort(const KParams& p, bool debug, const float4* x, const float4* vw
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
         const int b = team_blocks(p.n, L, p.block);
         if (debug)
-            k_vort<true, L, V><<<b, p.block, 0, st>>>(p, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort,
-                                                      visc, cell, ticket, hist, err);
+            k_vort<true, L, V><<<pass_grid(p, k_vort<true, L, V>, b), p.block, 0, st>>>(
+                p, b, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort, visc, cell, ticket, hist, err);
         else
-            k_vort<false, L, V><<<b, p.block, 0, st>>>(p, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out,
-                                                       vort, visc, cell, ticket, hist, err);
+            k_vort<false, L, V><<<pass_grid(p, k_vort<false, L, V>, b), p.block, 0, st>>>(
+                p, b, x, vw, omega, nbr, ncnt, xout, vout, perm_in, perm_out, vort, visc, cell, ticket, hist, err);
     });
 }
 

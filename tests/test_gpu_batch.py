@@ -95,3 +95,23 @@ def test_batch_stats_and_density_error():
         worst = max(worst, mx)
         off += sc.n
     assert abs(st["max_density_error"] - worst) <= 1e-4
+
+
+@pytest.mark.parametrize("lanes,cell_scale", [(2, 1.0), (1, 0.5), (4, 0.5)])
+def test_persistent_passes_bitexact(lanes, cell_scale):
+    """Each neighbour pass as one persistent launch (the resident blocks stride
+    over every scene's tiles of slots) gives the oracle's results bit for bit,
+    like the one-block-per-tile launch, in the adaptive loop too."""
+    scs = scenes.config2(seed=7, n_scenes=5, lo=800, hi=5000)
+    for sc in scs:
+        sc.ext_overrides["grid_dims"] = [int(round(d / cell_scale)) for d in sc.ext_overrides["grid_dims"]]
+    ext = dict(persistent=1, pair_lanes=lanes, cell_scale=cell_scale, block_size=128)
+    b = run_batch(scs, 3, **ext)
+    for i, sc in enumerate(scs):
+        check_scene_vs_oracle(b, i, sc, 3, pair_lanes=lanes, cell_scale=cell_scale)
+    ad = run_batch(scs, 2, adaptive=1, density_tol=0.02, max_iterations=8, **ext)
+    plain = run_batch(scs, 2, adaptive=1, density_tol=0.02, max_iterations=8, pair_lanes=lanes,
+                      cell_scale=cell_scale, block_size=128)
+    assert ad.stats()["total_iterations"] == plain.stats()["total_iterations"]
+    for name in ("x", "v"):
+        assert np.array_equal(ad.fetch(name).view(np.uint32), plain.fetch(name).view(np.uint32)), name

@@ -186,3 +186,31 @@ def test_collect_batch_rows():
     assert np.isfinite(f).all() and np.isfinite(t).all()
     assert (f[:, 0] >= 0).all() and (f[:, 0] <= 1).all()
     assert np.abs(t).max() > 0
+
+
+@pytest.mark.parametrize("lanes,block,persistent,clamp", [(2, 256, 0, 4.0), (2, 256, 1, 0.0), (1, 128, 0, 4.0),
+                                                          (4, 256, 0, 0.0), (2, 64, 1, 4.0)])
+def test_fused_warm_pass_matches_the_two_launch_path(lanes, block, persistent, clamp):
+    """The fused first pass (features on chip, the network on the tensor cores in
+    the same kernel) gives the two-launch path's lambda0, total lambda and state
+    bit for bit over several substeps, for every tile shape (256, 128 or 64 rows
+    per block: two, one or a partial MMA tile)."""
+    sc = scenes.dam_break(20, (40, 20, 20), stable=True, iterations=2)
+    feat, target = learned.collect(sc, substeps=30, rows_per_substep=2048, seed=0)
+    tr, _ = learned.train(feat, target, epochs=1, batch=2048, lr=2e-3)
+    _, b32, w16 = tr.params()
+    tr.close()
+    ext = dict(warm_start=1, pair_lanes=lanes, block_size=block, persistent=persistent, warm_clamp=clamp,
+               record_features=1)
+    runs = []
+    for unfused in (0, 1):
+        s = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(warm_unfused=unfused, **ext))
+        learned.install(s, w16, b32)
+        s.upload(sc.pos, sc.vel)
+        s.step(4)
+        assert s.stats()["error_bits"] == 0
+        runs.append({k: s.fetch(k) for k in ("lambda0", "lambda_total", "x", "v", "features")})
+        s.close()
+    for k in runs[0]:
+        assert np.array_equal(runs[0][k].view(np.uint32), runs[1][k].view(np.uint32)), k
+    assert np.abs(runs[0]["lambda0"]).max() > 0
