@@ -96,7 +96,9 @@ typedef struct pbf_ext_params {
                             features through HBM (default 0: one fused launch, the features go
                             from the feature pass to the tensor cores through shared memory).
                             Same results; kept for measurement */
-    int reserved[1];
+    int warm_floor;      /* 1: with warm_clamp > 0, lambda0 is also at least as strong as the plain
+                            lambda of its pass (between it and warm_clamp times it), so the first
+                            correction never pushes less than a plain iteration would (default 0) */
 } pbf_ext_params;
 
 typedef struct pbf_stats {

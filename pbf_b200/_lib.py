@@ -59,7 +59,7 @@ class ExtParams(C.Structure):
         ("cell_order", C.c_int), ("flags", C.c_uint), ("scorr_scale", C.c_float),
         ("sphere", C.c_float * 4), ("adaptive", C.c_int), ("density_tol", C.c_float),
         ("max_iterations", C.c_int), ("measure_error", C.c_int), ("debug", C.c_int),
-        ("warm_start", C.c_int), ("profile", C.c_int), ("block_size", C.c_int), ("record_features", C.c_int), ("warm_clamp", C.c_float), ("pair_lanes", C.c_int), ("persistent", C.c_int), ("warm_unfused", C.c_int), ("reserved", C.c_int * 1),
+        ("warm_start", C.c_int), ("profile", C.c_int), ("block_size", C.c_int), ("record_features", C.c_int), ("warm_clamp", C.c_float), ("pair_lanes", C.c_int), ("persistent", C.c_int), ("warm_unfused", C.c_int), ("warm_floor", C.c_int),
     ]
 
 

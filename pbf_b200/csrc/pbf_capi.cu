@@ -312,6 +312,9 @@ int validate(const pbf_solver_parameter* p, const float* gs, const float* bd, co
         return fail(PBF_ERR_INVALID, "pair_lanes must be 0, 1, 2, 4 or 8");
     if (e->persistent != 0 && e->persistent != 1) return fail(PBF_ERR_INVALID, "persistent must be 0 or 1");
     if (e->warm_unfused != 0 && e->warm_unfused != 1) return fail(PBF_ERR_INVALID, "warm_unfused must be 0 or 1");
+    if (e->warm_floor != 0 && e->warm_floor != 1) return fail(PBF_ERR_INVALID, "warm_floor must be 0 or 1");
+    if (e->warm_floor && e->warm_clamp > 0.0f && e->warm_clamp < 1.0f)
+        return fail(PBF_ERR_INVALID, "warm_floor needs warm_clamp >= 1 (or 0)");
     return PBF_OK;
 }
 
@@ -440,7 +443,7 @@ int enqueue_substep(pbf_solver* s, cudaStream_t st) {
             P(ST_LAMBDA, [&] {
                 rc = launch_features_warm(kp, s->Px, s->Pv, s->nbr, s->ncnt, s->lam_prev_sorted, s->Q,
                                           s->ext.record_features ? s->feat : nullptr, s->lam_acc, s->mlp_w, s->mlp_b,
-                                          s->lam0, s->ext.warm_clamp, err, st);
+                                          s->lam0, s->ext.warm_clamp, s->ext.warm_floor, err, st);
             });
             if (rc) return fail(PBF_ERR_CUDA, "fused warm-start pass: launch configuration failed");
         } else {
@@ -449,7 +452,8 @@ int enqueue_substep(pbf_solver* s, cudaStream_t st) {
             });
             if (warm)
                 P(ST_MLP, [&] {
-                    mlp_infer(s->mlp_w, s->mlp_b, s->feat, n, s->lam0, s->Q, s->lam_acc, s->ext.warm_clamp, err, st);
+                    mlp_infer(s->mlp_w, s->mlp_b, s->feat, n, s->lam0, s->Q, s->lam_acc, s->ext.warm_clamp,
+                              s->ext.warm_floor, err, st);
                 });
         }
         const bool last = !s->ext.adaptive && iters == 1;
@@ -1286,7 +1290,7 @@ int pbf_mlp_forward(pbf_mlp_trainer* tr, const float* d_feat, int batch, float* 
     if (!d_err) CK(cudaMalloc(&d_err, sizeof(int)));
     cudaStream_t st = (cudaStream_t)stream;
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-    if (mlp_infer(mlp_weights_bf16(tr->t), mlp_biases(tr->t), d_feat, batch, d_out, nullptr, nullptr, 0.0f, d_err,
+    if (mlp_infer(mlp_weights_bf16(tr->t), mlp_biases(tr->t), d_feat, batch, d_out, nullptr, nullptr, 0.0f, 0, d_err,
                   st))
         return fail(PBF_ERR_CUDA, "inference kernel failed");
     int h = 0;

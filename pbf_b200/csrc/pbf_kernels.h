@@ -39,7 +39,7 @@ void launch_features(const KParams& p, const float4* x, const float4* v, const i
 // when not null). Returns nonzero when the launch could not be configured.
 int launch_features_warm(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
                          const float* lam_prev, float4* xl, float* feat, float* lam_acc, const uint16_t* w,
-                         const float* b, float* lam0, float clamp, int* err, cudaStream_t st);
+                         const float* b, float* lam0, float clamp, int floor, int* err, cudaStream_t st);
 void launch_gather_rows(const int* slots, int count, int n, const float* feat, const float* lam_acc, float* out_feat,
                         float* out_target, int* err, cudaStream_t st);
 void launch_count_fallback(const int* iters, int first, int configured, int* fallback, long long* total,

@@ -101,6 +101,7 @@ struct FwdIO {
     float4* q;
     float* lam_acc;
     float clamp;  // trust-region factor around q.w (0: none)
+    int floor;    // 1: lambda0 at least as strong as q.w (same sign, magnitude >= |q.w|)
     // training
     const float* target;  // [n]
     float inv_batch;
@@ -278,7 +279,8 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
                     // same sign, at most clamp times its magnitude
                     const float lp = reinterpret_cast<const float*>(io.q)[4 * (size_t)row + 3];
                     const float a = io.clamp * lp;
-                    lam0 = fminf(fmaxf(lam0, fminf(a, 0.0f)), fmaxf(a, 0.0f));
+                    const float f0 = io.floor ? lp : 0.0f;  // the weak end of the interval
+                    lam0 = fminf(fmaxf(lam0, fminf(a, f0)), fmaxf(a, f0));
                 }
                 if (io.out) io.out[row] = lam0;
                 if (io.q) reinterpret_cast<float*>(io.q)[4 * (size_t)row + 3] = lam0;
@@ -462,7 +464,7 @@ static int sm_count() {
 }
 
 int mlp_infer(const uint16_t* w_bf16, const float* b, const float* feat, int n, float* out, float4* q, float* lam_acc,
-              float clamp, int* err, cudaStream_t st) {
+              float clamp, int floor, int* err, cudaStream_t st) {
     if (n <= 0) return 0;
     static bool attr = false;
     if (!attr) {
@@ -480,6 +482,7 @@ int mlp_infer(const uint16_t* w_bf16, const float* b, const float* feat, int n, 
     io.q = q;
     io.lam_acc = lam_acc;
     io.clamp = clamp;
+    io.floor = floor;
     io.err = err;
     // four CTAs per SM (54 KB of shared memory and 128 TMEM columns each) overlap
     // one another's tensor-core waits

@@ -40,9 +40,10 @@ int tc_gemm_bf16(const void* A, const void* B, float* D, int N, int K, int* err,
 // Inference: lambda0 for `n` rows of raw features feat[n][12]. Writes lambda0 to
 // out (if not null), to q[k].w (if not null) and to lam_acc (if not null). With q
 // and clamp > 0, lambda0 is kept to the sign of the plain lambda in q[k].w and
-// to at most clamp times its magnitude.
+// to at most clamp times its magnitude (and, with floor, to at least its
+// magnitude).
 int mlp_infer(const uint16_t* w_bf16, const float* b, const float* feat, int n, float* out, float4* q,
-              float* lam_acc, float clamp, int* err, cudaStream_t st);
+              float* lam_acc, float clamp, int floor, int* err, cudaStream_t st);
 // failure injection (tests): the same kernel with no MMA committed to its
 // barrier, each wait limited to wait_limit polls
 int mlp_infer_uncommitted(const uint16_t* w_bf16, const float* b, const float* feat, int n, float* out,

@@ -460,6 +460,7 @@ struct WarmIO {
     const float* b;     // biases and constants (normalisation, output scale)
     float* lam0;        // lambda0 per slot
     float clamp;        // trust region around the plain lambda (0: none)
+    int floor;          // 1: lambda0 at least as strong as the plain lambda
     int* err;           // PBF_DEVERR_MLP_TIMEOUT on an expired tensor-core wait
 };
 
@@ -580,7 +581,8 @@ __global__ void __launch_bounds__(256, 3) k_features_warm(KParams p, int nvb, co
                 // trust region around the plain lambda of this pass: same sign,
                 // at most clamp times its magnitude
                 const float a = io.clamp * s_lam[t];
-                l0 = fminf(fmaxf(l0, fminf(a, 0.0f)), fmaxf(a, 0.0f));
+                const float f0 = io.floor ? s_lam[t] : 0.0f;  // the weak end of the interval
+                l0 = fminf(fmaxf(l0, fminf(a, f0)), fmaxf(a, f0));
             }
             reinterpret_cast<float*>(xl)[4 * (size_t)k + 3] = l0;
             lam_acc[k] = l0;
@@ -923,7 +925,7 @@ void launch_features(const KParams& p, const float4* x, const float4* v, const i
 
 int launch_features_warm(const KParams& p, const float4* x, const float4* v, const int* nbr, const int* ncnt,
                          const float* lam_prev, float4* xl, float* feat, float* lam_acc, const uint16_t* w,
-                         const float* b, float* lam0, float clamp, int* err, cudaStream_t st) {
+                         const float* b, float* lam0, float clamp, int floor, int* err, cudaStream_t st) {
     int rc = 0;
     with_lanes(p.lanes, [&](auto c) {
         constexpr int L = decltype(c)::L, V = decltype(c)::V;
@@ -945,7 +947,7 @@ int launch_features_warm(const KParams& p, const float4* x, const float4* v, con
                 per_sm = 1;
             grid = (int)std::min<long long>((long long)per_sm * sms, nvb);
         }
-        const WarmIO io{w, b, lam0, clamp, err};
+        const WarmIO io{w, b, lam0, clamp, floor, err};
         k_features_warm<L, V><<<grid, p.block, smem, st>>>(p, nvb, x, v, nbr, ncnt, lam_prev, xl, feat, lam_acc, io);
     });
     return rc;

@@ -188,9 +188,10 @@ def test_collect_batch_rows():
     assert np.abs(t).max() > 0
 
 
-@pytest.mark.parametrize("lanes,block,persistent,clamp", [(2, 256, 0, 4.0), (2, 256, 1, 0.0), (1, 128, 0, 4.0),
-                                                          (4, 256, 0, 0.0), (2, 64, 1, 4.0)])
-def test_fused_warm_pass_matches_the_two_launch_path(lanes, block, persistent, clamp):
+@pytest.mark.parametrize("lanes,block,persistent,clamp,floor", [(2, 256, 0, 4.0, 0), (2, 256, 1, 0.0, 0),
+                                                                (1, 128, 0, 4.0, 1), (4, 256, 0, 0.0, 0),
+                                                                (2, 64, 1, 4.0, 1)])
+def test_fused_warm_pass_matches_the_two_launch_path(lanes, block, persistent, clamp, floor):
     """The fused first pass (features on chip, the network on the tensor cores in
     the same kernel) gives the two-launch path's lambda0, total lambda and state
     bit for bit over several substeps, for every tile shape (256, 128 or 64 rows
@@ -201,7 +202,7 @@ def test_fused_warm_pass_matches_the_two_launch_path(lanes, block, persistent, c
     _, b32, w16 = tr.params()
     tr.close()
     ext = dict(warm_start=1, pair_lanes=lanes, block_size=block, persistent=persistent, warm_clamp=clamp,
-               record_features=1)
+               warm_floor=floor, record_features=1)
     runs = []
     for unfused in (0, 1):
         s = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext(warm_unfused=unfused, **ext))
@@ -214,3 +215,31 @@ def test_fused_warm_pass_matches_the_two_launch_path(lanes, block, persistent, c
     for k in runs[0]:
         assert np.array_equal(runs[0][k].view(np.uint32), runs[1][k].view(np.uint32)), k
     assert np.abs(runs[0]["lambda0"]).max() > 0
+
+
+def test_trust_region_floor_keeps_lambda0_between_the_plain_lambda_and_its_multiple():
+    """With warm_floor, lambda0 lies between the plain lambda of its pass and
+    warm_clamp times it: the first correction never pushes less than a plain
+    iteration would. The plain lambda is that of a solver without the warm start
+    stepped once from the same upload (one correction: its total lambda)."""
+    sc = scenes.dam_break(16, (40, 20, 20), stable=True, iterations=2)
+    feat, target = learned.collect(sc, substeps=20, rows_per_substep=1024, seed=0)
+    tr, _ = learned.train(feat, target, epochs=1, batch=1024, lr=2e-3)
+    _, b32, w16 = tr.params()
+    tr.close()
+    sc1 = scenes.dam_break(16, (40, 20, 20), stable=True, iterations=1)
+    warm = Solver(sc1.para, sc1.grid_space, sc1.boundary, sc1.ext(warm_start=1, warm_clamp=3.0, warm_floor=1))
+    learned.install(warm, w16, b32)
+    plain = Solver(sc1.para, sc1.grid_space, sc1.boundary, sc1.ext(record_features=1))
+    for s in (warm, plain):
+        s.upload(sc1.pos, sc1.vel)
+        s.step(1)
+    l0 = warm.fetch("lambda0")
+    lp = plain.fetch("lambda_total")
+    assert np.array_equal(warm.fetch("perm"), plain.fetch("perm"))
+    lo = np.minimum(lp, np.float32(3.0) * lp)
+    hi = np.maximum(lp, np.float32(3.0) * lp)
+    assert np.all(l0 >= lo) and np.all(l0 <= hi)
+    assert np.count_nonzero(lp) > 0 and np.count_nonzero(l0 != lp) > 0
+    warm.close()
+    plain.close()
