@@ -215,6 +215,8 @@ def run_reference(args) -> int:
     line = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "impl": "reference", "scaling": "weak", "dtype": "f32",
             "data": "synthetic", "config": workload_config(args)}
+    line["config"]["workload"] = line["config"]["workload"].replace("stable mode", "the reference CPU solver's own "
+                                                                    "formulas (src/solver.cpp)")
     line["config"]["formulas"] = "the reference's own (src/solver.cpp); the GPU arm runs the stable mode"
     if not O.refcpu_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver not built (oracle/_ref missing)"}))
@@ -558,7 +560,11 @@ def _timed_errors(solver, steps, flush, stream, barrier, max_over_ranks):
 # lambda those iterations apply), and the trust region factor (0: none).
 LEARN_COLLECT_ITERS = 4
 LEARN_CLAMP = 4.0
+LEARN_FLOOR = 1
 LEARN_CORRECTIONS = 2
+# common max-error tolerances at which both solvers run adaptively (each
+# substep iterates until its max one-sided error is within the tolerance)
+LEARN_TOLERANCES = (0.1, 0.05)
 
 
 def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, plain, plain_batched) -> dict:
@@ -587,12 +593,13 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
     out = {"training": {"substeps": 2000, "collect_iterations": LEARN_COLLECT_ITERS, "rows": 2000 * 2048,
                         "epochs": 3, "batch": 4096, "loss_first": losses[0][1], "loss_last": losses[-1][1],
                         "collect_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2)},
-           "corrections": LEARN_CORRECTIONS, "warm_clamp": LEARN_CLAMP}
+           "corrections": LEARN_CORRECTIONS, "warm_clamp": LEARN_CLAMP, "warm_floor": LEARN_FLOOR}
 
     def single(iters, warm, **kw):
         sc = scenes.config1(seed=rank, iterations=iters)
         s = Solver(sc.para, sc.grid_space, sc.boundary,
-                   sc.ext(warm_start=1 if warm else 0, warm_clamp=LEARN_CLAMP, **ext_kw, **kw))
+                   sc.ext(warm_start=1 if warm else 0, warm_clamp=LEARN_CLAMP, warm_floor=LEARN_FLOOR, **ext_kw,
+                          **kw))
         if warm:
             learned.install(s, w16, b32)
         s.upload(sc.pos, sc.vel)
@@ -617,7 +624,7 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
         para, descs, ov, pos, vel = scenes.batch_inputs(mine, iterations=iters)
         for d in descs:
             d["grid_dims"] = autotune.dims_for_scale(d["grid_dims"], bt["cell_scale"])
-        ov.update(bt, warm_start=1 if warm else 0, warm_clamp=LEARN_CLAMP, **kw)
+        ov.update(bt, warm_start=1 if warm else 0, warm_clamp=LEARN_CLAMP, warm_floor=LEARN_FLOOR, **kw)
         b = BatchSolver(para, descs, scenes.default_ext(**ov))
         if warm:
             learned.install(b, w16, b32)
@@ -648,6 +655,15 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
     out["learned_batched_at_plain_error"] = batch(1, True, **adapt(e_pb))
     # learned + batched against the plain single scene at the learned batch's error
     out["plain_single_at_learned_batch_error"] = single(1, False, **adapt(e_lb))
+    # both solvers adaptive to the same tight tolerances, on config 3 and on the batch
+    out["at_tolerance"] = {}
+    for tol in LEARN_TOLERANCES:
+        r = {"single_learned": single(1, True, **adapt(tol)), "single_plain": single(1, False, **adapt(tol)),
+             "batch_learned": batch(1, True, **adapt(tol)), "batch_plain": batch(1, False, **adapt(tol))}
+        r["speedup_single"] = r["single_learned"]["value"] / r["single_plain"]["value"]
+        r["speedup_batch"] = r["batch_learned"]["value"] / r["batch_plain"]["value"]
+        r["speedup_learned_batched_vs_plain_single"] = r["batch_learned"]["value"] / r["single_plain"]["value"]
+        out["at_tolerance"][str(tol)] = r
     out["speedup"] = {
         "config3_at_learned_error": out["single"]["value"] / out["plain_at_learned_error"]["value"],
         "config3_at_plain4_error": out["learned_at_plain_error"]["value"] / plain["value"],
@@ -673,8 +689,8 @@ def measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, wei
     w16, b32 = weights
     legs = [("plain", 4, {})]
     for label, iters, kw in legs + [("plain_adaptive", 2, {"adaptive": 1, "max_iterations": 16}),
-                                    ("learned_adaptive", 2, {"warm_start": 1, "adaptive": 1,
-                                                             "max_iterations": 16})]:
+                                    ("learned_adaptive", 2, {"warm_start": 1, "warm_floor": LEARN_FLOOR,
+                                                             "adaptive": 1, "max_iterations": 16})]:
         if kw.get("adaptive"):
             kw = dict(kw, density_tol=out["plain"]["density_error"]["max"])
         scs = scenes.config4(seed=0, iterations=iters)
