@@ -450,12 +450,21 @@ public:
 
     // ---- one substep ----------------------------------------------------------
     void predict() {
-        // updateParticles kernels/cudaPBFSolver.cu:4-13; CPU src/solver.cpp:63-69
+        // updateParticles kernels/cudaPBFSolver.cu:4-13; CPU src/solver.cpp:63-69.
+        // GPU formulation: v += dt g and x += dt v each round once, as fused
+        // multiply-adds (nvcc contracts these lines of the reference by default;
+        // the library evaluates the same fma). CPU formulation: a product and a
+        // sum (g++ without -mfma does not contract).
         const V3<T> g{(T)p.gravity[0], (T)p.gravity[1], (T)p.gravity[2]};
         for (int i = 0; i < n; ++i) {
             xold[i] = x[i];
-            v[i] = {v[i].x + k.dt * g.x, v[i].y + k.dt * g.y, v[i].z + k.dt * g.z};
-            x[i] = {x[i].x + k.dt * v[i].x, x[i].y + k.dt * v[i].y, x[i].z + k.dt * v[i].z};
+            if (p.formulation == 0) {
+                v[i] = {std::fma(k.dt, g.x, v[i].x), std::fma(k.dt, g.y, v[i].y), std::fma(k.dt, g.z, v[i].z)};
+                x[i] = {std::fma(k.dt, v[i].x, x[i].x), std::fma(k.dt, v[i].y, x[i].y), std::fma(k.dt, v[i].z, x[i].z)};
+            } else {
+                v[i] = {v[i].x + k.dt * g.x, v[i].y + k.dt * g.y, v[i].z + k.dt * g.z};
+                x[i] = {x[i].x + k.dt * v[i].x, x[i].y + k.dt * v[i].y, x[i].z + k.dt * v[i].z};
+            }
             bound(x[i]);
             xpred[i] = x[i];
         }

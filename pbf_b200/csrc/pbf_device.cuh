@@ -265,10 +265,16 @@ __device__ __forceinline__ float wall_term(const KParams& p, const SceneView& sc
     return rho;
 }
 
-// updateParticles (cu:4-13): v += dt g; x += dt v; bound
+// updateParticles (cu:4-13): v += dt g; x += dt v; bound. Each update is one
+// fused multiply-add, fma(dt, g, v) and fma(dt, v, x): the single rounding the
+// reference's own build gives these two lines (nvcc contracts a product that
+// feeds an add by default). With two roundings, a predicted position could sit
+// one ulp from the reference's, which flips the neighbour-list membership of
+// pairs at exactly h, and such a pair then acts for every Jacobi iteration once
+// the corrections bring it within h.
 __device__ __forceinline__ void predict(const KParams& p, const SceneView& sc, f3& x, f3& v) {
-    v = {v.x + p.dt * p.g[0], v.y + p.dt * p.g[1], v.z + p.dt * p.g[2]};
-    x = {x.x + p.dt * v.x, x.y + p.dt * v.y, x.z + p.dt * v.z};
+    v = {__fmaf_rn(p.dt, p.g[0], v.x), __fmaf_rn(p.dt, p.g[1], v.y), __fmaf_rn(p.dt, p.g[2], v.z)};
+    x = {__fmaf_rn(p.dt, v.x, x.x), __fmaf_rn(p.dt, v.y, x.y), __fmaf_rn(p.dt, v.z, x.z)};
     bound_particle(p, sc, x);
 }
 
