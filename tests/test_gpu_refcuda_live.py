@@ -19,7 +19,14 @@ double-precision sine of its own, and the offset is a fractional part of
 sin(...) * 43758.5453, so one ulp of the sine moves it anywhere in
 [0, RANDOM_OFFSET_COEFF). With one clamped axis the clamped position differs by
 at most 0.01 (include/solverBase.h:5); four Jacobi iterations spread that into
-the particle and its neighbours, bounded here at 4 x 0.01.
+the particle's neighbours, bounded here at 4 x 0.01 (measured on the floor
+layer of scene 1 moving down: at most 0.0098 for the 4,096 clamped particles
+and 0.031 for any particle).
+
+The library's prediction v += dt g, x += dt v rounds each update once (a fused
+multiply-add), as the reference's build of those lines does; with two
+roundings, pairs at exactly h left the neighbour list in one solver and not the
+other, and such a pair acts for every later Jacobi iteration.
 """
 import os
 
@@ -108,10 +115,13 @@ def test_wall_clamped_particles_within_the_offset_bound():
     xp = sc.pos + dt * v1
     lo, hi = np.float32(sc.boundary[:3]), np.float32(sc.boundary[3:])
     clamped = ((xp < lo) | (xp > hi)).any(1)
-    assert clamped.sum() > 5000
+    assert clamped.sum() >= 4096  # the whole bottom layer of the 64^3 lattice
     d = np.abs(ours["x"].astype(np.float64) - ra["x"].astype(np.float64)).max(1)
-    assert d[clamped].max() <= 4 * RANDOM_OFFSET_COEFF, d[clamped].max()
+    # the clamped particles themselves: within the offset range (measured 0.0098)
+    assert d[clamped].max() <= 2 * RANDOM_OFFSET_COEFF, d[clamped].max()
     assert np.quantile(d[clamped], 0.99) <= RANDOM_OFFSET_COEFF
+    # their neighbours, through four Jacobi iterations (measured 0.031)
+    assert d.max() <= 4 * RANDOM_OFFSET_COEFF, d.max()
     # every particle stays inside the walls in both
     for x in (ours["x"], ra["x"]):
         assert (x >= lo - 1e-5).all() and (x <= hi + 1e-5).all()
