@@ -12,8 +12,9 @@ reference's literal parameters (gravity -49 as in kernels/cudaPBFSolver.cu:9).
 * floating-point fields are compared away from the walls: the wall clamp hashes
   positions through sinf(...) * 43758.5453 (cuh:116-119), which turns an ulp of
   difference into a different offset, so clamped particles and their neighbours
-  differ by design. With one iteration every interior field agrees to 2e-5 of
-  its scale. With four iterations at these (diverging) parameters the interior
+  differ by design. With one iteration every interior field agrees to 1e-5 of
+  its scale (x 1e-7, lambda 4e-7, dp 2e-6, v 3e-6, vorticity 8e-6; the
+  prediction rounds once per update, as the reference's build contracts it). With four iterations at these (diverging) parameters the interior
   is reached by the wall differences, so only the integer stages are compared.
 """
 import os
@@ -73,4 +74,4 @@ def test_interior_fields_match_reference_cuda_one_iteration():
         assert m.sum() > 800
         d = np.abs(ref - got)
         d = d.max(1) if d.ndim > 1 else d
-        assert d[m].max() <= 2e-5 * np.abs(ref).max(), (name, d[m].max() / np.abs(ref).max())
+        assert d[m].max() <= 1e-5 * np.abs(ref).max(), (name, d[m].max() / np.abs(ref).max())
