@@ -564,7 +564,8 @@ LEARN_FLOOR = 1
 LEARN_CORRECTIONS = 2
 # common max-error tolerances at which both solvers run adaptively (each
 # substep iterates until its max one-sided error is within the tolerance)
-LEARN_TOLERANCES = (0.1, 0.05)
+LEARN_TOLERANCES = (0.1, 0.05, 0.03)
+WARM_BLOCK = 256
 
 
 def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, plain, plain_batched) -> dict:
@@ -595,11 +596,17 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
                         "collect_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2)},
            "corrections": LEARN_CORRECTIONS, "warm_clamp": LEARN_CLAMP, "warm_floor": LEARN_FLOOR}
 
+    # The fused warm pass runs two 128-row MMA tiles per block of 256 threads and
+    # stages the network's weights once per block: warm-started solvers take
+    # 256-thread blocks; plain ones keep the autotuner's choice.
+    def launch(kw, warm):
+        return dict(kw, block_size=WARM_BLOCK) if warm else dict(kw)
+
     def single(iters, warm, **kw):
         sc = scenes.config1(seed=rank, iterations=iters)
         s = Solver(sc.para, sc.grid_space, sc.boundary,
-                   sc.ext(warm_start=1 if warm else 0, warm_clamp=LEARN_CLAMP, warm_floor=LEARN_FLOOR, **ext_kw,
-                          **kw))
+                   sc.ext(warm_start=1 if warm else 0, warm_clamp=LEARN_CLAMP, warm_floor=LEARN_FLOOR,
+                          **launch(ext_kw, warm), **kw))
         if warm:
             learned.install(s, w16, b32)
         s.upload(sc.pos, sc.vel)
@@ -624,7 +631,8 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
         para, descs, ov, pos, vel = scenes.batch_inputs(mine, iterations=iters)
         for d in descs:
             d["grid_dims"] = autotune.dims_for_scale(d["grid_dims"], bt["cell_scale"])
-        ov.update(bt, warm_start=1 if warm else 0, warm_clamp=LEARN_CLAMP, warm_floor=LEARN_FLOOR, **kw)
+        ov.update(launch(bt, warm), warm_start=1 if warm else 0, warm_clamp=LEARN_CLAMP, warm_floor=LEARN_FLOOR,
+                  **kw)
         b = BatchSolver(para, descs, scenes.default_ext(**ov))
         if warm:
             learned.install(b, w16, b32)
@@ -690,6 +698,7 @@ def measure_large(args, rank, world, flush, stream, barrier, max_over_ranks, wei
     legs = [("plain", 4, {})]
     for label, iters, kw in legs + [("plain_adaptive", 2, {"adaptive": 1, "max_iterations": 16}),
                                     ("learned_adaptive", 2, {"warm_start": 1, "warm_floor": LEARN_FLOOR,
+                                                             "warm_clamp": LEARN_CLAMP,
                                                              "adaptive": 1, "max_iterations": 16})]:
         if kw.get("adaptive"):
             kw = dict(kw, density_tol=out["plain"]["density_error"]["max"])
