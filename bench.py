@@ -559,7 +559,7 @@ def _timed_errors(solver, steps, flush, stream, barrier, max_over_ranks):
 # with LEARN_COLLECT_ITERS Jacobi iterations per substep (the target is the total
 # lambda those iterations apply), and the trust region factor (0: none).
 LEARN_COLLECT_ITERS = 4
-LEARN_CLAMP = 8.0
+LEARN_CLAMP = 16.0
 LEARN_FLOOR = 1
 LEARN_CORRECTIONS = 2
 # common max-error tolerances at which both solvers run adaptively (each
