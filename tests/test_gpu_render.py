@@ -84,3 +84,37 @@ def test_render_rejects_bad_arguments():
     import torch
     with pytest.raises(PBFError):
         r.frame(cam, positions=torch.zeros((4, 3), device="cuda"), stride=3)
+
+
+@pytest.mark.gpu
+def test_render_known_answers_on_the_gpu():
+    """The closed forms of tests/test_render_pins.py straight through the CUDA
+    passes: two overlapping sprites (sphere fronts under the depth test, chords
+    summed) and the room seen head-on from inside."""
+    import torch
+    from test_render_pins import _room_centre, _sphere_profile, _sprite_camera
+    w = h = 129
+    dist = 5.0
+    cam = _sprite_camera(w, h, dist, 0.5)
+    second = (0.6, 0.1, -0.3)
+    pos = np.array([[0.0, 0.0, 0.0], second], np.float32)
+    r = render.Renderer(w, h)
+    r.frame(cam, positions=torch.from_numpy(pos).cuda(), stride=3)
+    z, th = r.read("depth_raw"), r.read("thickness")
+    r.close()
+    c1, q1, d1, t1 = _sphere_profile(cam, w, h)
+    c2, q2, d2, t2 = _sphere_profile(cam, w, h, second)
+    inside = ((q1 < 0.99) | (q1 > 1.01)) & ((q2 < 0.99) | (q2 > 1.01))
+    want_z = np.where(c1 & c2, np.minimum(d1, d2), np.where(c1, d1, np.where(c2, d2, 0.0)))
+    want_t = np.where(c1, t1, 0.0) + np.where(c2, t2, 0.0)
+    assert np.abs(z[inside] - want_z[inside]).max() <= 2e-6 * dist
+    assert np.abs(th[inside] - want_t[inside]).max() <= 1e-5
+    # the room: the back wall head-on, lit by the light above the room's centre
+    w = h = 33
+    cam = render.make_camera((0.0, 25.0, 20.0), (0.0, 25.0, -30.0), (0, 1, 0), math.radians(40.0), w, h, 0.1)
+    r = render.Renderer(w, h)
+    r.frame(cam, positions=torch.zeros((1, 3), device="cuda") + 1000.0, stride=3)  # no particle in view
+    got = r.read("room")[h // 2, w // 2]
+    r.close()
+    assert np.array_equal(got, _room_centre((0.0, 25.0, 20.0), (0.0, 25.0, -30.0), (0, 1, 0)))
+    assert np.all(got[:3] == np.float32(200.0 / 255.0))
