@@ -596,11 +596,11 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
                         "collect_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2)},
            "corrections": LEARN_CORRECTIONS, "warm_clamp": LEARN_CLAMP, "warm_floor": LEARN_FLOOR}
 
-    # The fused warm pass runs two 128-row MMA tiles per block of 256 threads and
-    # stages the network's weights once per block: warm-started solvers take
-    # 256-thread blocks; plain ones keep the autotuner's choice.
+    # The fused warm pass stages the network's weights once per block and runs
+    # 128-row MMA tiles: warm-started solvers take 256-thread blocks, one block
+    # per tile of slots; plain ones keep the autotuner's choice.
     def launch(kw, warm):
-        return dict(kw, block_size=WARM_BLOCK) if warm else dict(kw)
+        return dict(kw, block_size=WARM_BLOCK, persistent=0) if warm else dict(kw)
 
     def single(iters, warm, **kw):
         sc = scenes.config1(seed=rank, iterations=iters)

@@ -228,6 +228,26 @@ template <int V> __host__ __device__ constexpr int batches() { return 4 / V; }
 // a9: density, constraint and lambda (calculateLambda cu:156-180), with the
 // one-sided density error of the positions it sees
 // ---------------------------------------------------------------------------
+// Lambda of slot k from its combined fluid density and gradient sums: the wall
+// term, the constraint and the denominator. rhos gains the wall term; err is
+// the one-sided error of the fluid density alone.
+__device__ __forceinline__ float lambda_tail(const KParams& p, int k, const f3& xk, float& rhos, float gms, f3 g3,
+                                             float& err) {
+    err = fmaxf(__fdiv_rn(rhos, p.rho0) - 1.0f, 0.0f);
+    if (p.flags & FLAG_WALL_DENSITY) {
+        f3 gw;
+        rhos = rhos + wall_term(p, scene_of(p, k), xk, gw);
+        g3 = {g3.x + gw.x, g3.y + gw.y, g3.z + gw.z};
+    }
+    float C = __fdiv_rn(rhos, p.rho0) - 1.0f;
+    if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
+    gms = __fmaf_rn(g3.x, g3.x, gms);
+    gms = __fmaf_rn(g3.y, g3.y, gms);
+    gms = __fmaf_rn(g3.z, g3.z, gms);
+    gms = __fdiv_rn(gms, p.rho0sq);
+    return __fdiv_rn(-C, gms + p.eps);
+}
+
 template <bool DEBUG, int L, int V>
 __device__ __forceinline__ void lambda_tile(const KParams& p, int vb, const float4* __restrict__ x,
                                             const int* __restrict__ nbr, const int* __restrict__ ncnt,
@@ -267,23 +287,10 @@ __device__ __forceinline__ void lambda_tile(const KParams& p, int vb, const floa
             }
         }
         float rhos = team_sum<L>(fold(rho), tm.mask);
-        float gms = team_sum<L>(fold(gm), tm.mask);
-        f3 g3 = team_sum3<L>(fold3(gs), tm.mask);
+        const float gms = team_sum<L>(fold(gm), tm.mask);
+        const f3 g3 = team_sum3<L>(fold3(gs), tm.mask);
         if (tm.t == 0) {
-            // one-sided error of the fluid density at these positions (no wall term)
-            err = fmaxf(__fdiv_rn(rhos, p.rho0) - 1.0f, 0.0f);
-            if (p.flags & FLAG_WALL_DENSITY) {
-                f3 gw;
-                rhos = rhos + wall_term(p, scene_of(p, k), xk, gw);
-                g3 = {g3.x + gw.x, g3.y + gw.y, g3.z + gw.z};
-            }
-            float C = __fdiv_rn(rhos, p.rho0) - 1.0f;
-            if (p.flags & FLAG_CLAMP_C) C = fmaxf(C, 0.0f);
-            gms = __fmaf_rn(g3.x, g3.x, gms);
-            gms = __fmaf_rn(g3.y, g3.y, gms);
-            gms = __fmaf_rn(g3.z, g3.z, gms);
-            gms = __fdiv_rn(gms, p.rho0sq);
-            const float lam = __fdiv_rn(-C, gms + p.eps);
+            const float lam = lambda_tail(p, k, xk, rhos, gms, g3, err);
             xl[k] = make_float4(xk.x, xk.y, xk.z, lam);
             if (ctl.lam_acc) ctl.lam_acc[k] += lam;
             if (DEBUG) rho_out[k] = rhos;
@@ -535,9 +542,14 @@ __global__ void __launch_bounds__(256, 3) k_features_warm(KParams p, int nvb, co
         if (!alive) continue;  // an expired wait: no more tensor-core work (the error bit is set)
         // three hidden layers; layer l reads X (l = 0) or H and writes H (l < 2)
         float y = sb[B4_OFF];
+        // row t's plain lambda, read after the first barrier (its team leader
+        // wrote it) and before the second (after which that leader may write
+        // the next tile's)
+        float lam_plain = 0.0f;
 #pragma unroll 1
         for (int l = 0; l < 3; ++l) {
             sync_for_mma();
+            if (l == 0 && t < R) lam_plain = s_lam[t];
             if (t == 0) {
                 for (int j = 0; j < tiles; ++j) {
                     if (l == 0) gemm_issue(tbase + 64 * j, sX + j * FW_X_TILE, smem + FW_SW1, 64, 16, 0);
@@ -580,8 +592,8 @@ __global__ void __launch_bounds__(256, 3) k_features_warm(KParams p, int nvb, co
             if (io.clamp > 0.0f) {
                 // trust region around the plain lambda of this pass: same sign,
                 // at most clamp times its magnitude
-                const float a = io.clamp * s_lam[t];
-                const float f0 = io.floor ? s_lam[t] : 0.0f;  // the weak end of the interval
+                const float a = io.clamp * lam_plain;
+                const float f0 = io.floor ? lam_plain : 0.0f;  // the weak end of the interval
                 l0 = fminf(fmaxf(l0, fminf(a, f0)), fmaxf(a, f0));
             }
             reinterpret_cast<float*>(xl)[4 * (size_t)k + 3] = l0;

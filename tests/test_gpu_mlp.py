@@ -190,12 +190,12 @@ def test_collect_batch_rows():
 
 @pytest.mark.parametrize("lanes,block,persistent,clamp,floor", [(2, 256, 0, 4.0, 0), (2, 256, 1, 0.0, 0),
                                                                 (1, 128, 0, 4.0, 1), (4, 256, 0, 0.0, 0),
-                                                                (2, 64, 1, 4.0, 1)])
+                                                                (2, 64, 1, 4.0, 1), (1, 256, 0, 16.0, 1)])
 def test_fused_warm_pass_matches_the_two_launch_path(lanes, block, persistent, clamp, floor):
     """The fused first pass (features on chip, the network on the tensor cores in
     the same kernel) gives the two-launch path's lambda0, total lambda and state
-    bit for bit over several substeps, for every tile shape (256, 128 or 64 rows
-    per block: two, one or a partial MMA tile)."""
+    bit for bit over several substeps, for every tile shape (256, 128, 64 or 32
+    rows per block: two, one or a partial MMA tile)."""
     sc = scenes.dam_break(20, (40, 20, 20), stable=True, iterations=2)
     feat, target = learned.collect(sc, substeps=30, rows_per_substep=2048, seed=0)
     tr, _ = learned.train(feat, target, epochs=1, batch=2048, lr=2e-3)
