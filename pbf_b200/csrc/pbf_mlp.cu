@@ -6,6 +6,8 @@
 // 128-row tile, which is TMEM lane t of the accumulator, so each epilogue
 // (bias, GELU, its derivative, the output layer) is per-thread register work
 // on one particle after a tcgen05.ld of that thread's lane.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -91,6 +93,20 @@ int tc_gemm_bf16(const void* A, const void* B, float* D, int N, int K, int* err,
 // Forward pass over 128-row tiles (persistent CTAs). TRAIN additionally saves
 // what the backward pass needs and computes the output-layer gradients.
 // ---------------------------------------------------------------------------
+// Per-slot gradient partials of the training forward pass: loss, db4, dw4[64].
+constexpr int FWD_PART = 66;
+
+// out[i] = sum over parts p = 0, 1, ... of part[p * stride + i], in that order
+// (deterministic: the gradients are the same bits on every run)
+__global__ void k_sum_parts(const float* __restrict__ part, int nparts, int stride, int count,
+                            float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    float s = 0.0f;
+    for (int q = 0; q < nparts; ++q) s += part[(size_t)q * stride + i];
+    out[i] = s;
+}
+
 struct FwdIO {
     const uint16_t* w;   // bf16 weights
     const float* b;      // biases and constants
@@ -106,9 +122,7 @@ struct FwdIO {
     const float* target;  // [n]
     float inv_batch;
     uint16_t *x16, *h1, *h2, *g1, *g2, *dz3;  // [n][16] and [n][64] bf16
-    float* gw;                                 // gradient of the weights (w4 part written here)
-    float* gb;                                 // gradient of b4 written here
-    float* loss;
+    float* part;  // per tile and warp: loss, db4, dw4[64] (FWD_PART floats; summed by k_sum_parts)
     int* err;
     // failure injection (the bounded-wait test only): no MMA is issued or
     // committed, so every wait on the barrier runs out after wait_limit polls
@@ -296,15 +310,18 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(FwdIO io) {
                 l += __shfl_xor_sync(0xffffffffu, l, o);
                 db += __shfl_xor_sync(0xffffffffu, db, o);
             }
+            // this warp's sums go to its own slot; k_sum_parts adds the slots in a
+            // fixed order, so the gradients do not depend on the blocks' timing
+            float* slot = io.part + ((size_t)tile * 4 + warp) * FWD_PART;
             if (lane == 0) {
-                atomicAdd(io.loss, l);
-                atomicAdd(&io.gb[B4_OFF], db);
+                slot[0] = l;
+                slot[1] = db;
             }
             for (int nn = 0; nn < 64; ++nn) {
                 float gwn = dy * h3f[nn];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) gwn += __shfl_xor_sync(0xffffffffu, gwn, o);
-                if (lane == 0) atomicAdd(&io.gw[W4_OFF + nn], gwn);
+                if (lane == 0) slot[2 + nn] = gwn;
                 if (valid) {
                     const size_t at = (size_t)row * 64 + nn;
                     io.dz3[at] = bf16_bits(dy * sw4[nn] * bf16_val(io.dz3[at]));
@@ -329,8 +346,7 @@ struct BwdIO {
     const uint16_t* w;      // W [64][Kin]
     const uint16_t* gprev;  // [n][Kin] gelu' of the layer input, null for the first layer
     uint16_t* dz_prev;      // [n][Kin] out, null for the first layer
-    float* gw;              // [64][Kin] accumulated
-    float* gb;              // [64] accumulated
+    float* part;            // per tile: dW [64][Kin] then db [64] (summed by k_sum_parts)
     int n;
     int* err;
 };
@@ -391,7 +407,8 @@ __global__ void __launch_bounds__(128, 1) k_mlp_bwd(BwdIO io) {
             commit(&mbar);
         }
         if (!wait_mma(&mbar, phase, io.err)) break;
-        if (warp < 2) {  // rows 0..63 of the dW product: output unit m
+        if (warp < 2) {  // rows 0..63 of the dW product: output unit m, into this tile's slot
+            float* slot = io.part + (size_t)tile * (64 * KIN + 64);
 #pragma unroll 1
             for (int c = 0; c < NB / 16; ++c) {
                 float v[16];
@@ -400,8 +417,8 @@ __global__ void __launch_bounds__(128, 1) k_mlp_bwd(BwdIO io) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
                     const int k = 16 * c + i;
-                    if (k < KIN) atomicAdd(&io.gw[m * KIN + k], v[i]);
-                    else if (k == KIN) atomicAdd(&io.gb[m], v[i]);
+                    if (k < KIN) slot[m * KIN + k] = v[i];
+                    else if (k == KIN) slot[64 * KIN + m] = v[i];
                 }
             }
         }
@@ -516,6 +533,7 @@ struct MlpTrainer {
     int cap = 0;
     float *w32 = nullptr, *b32 = nullptr, *mw = nullptr, *vw = nullptr, *mb = nullptr, *vb = nullptr;
     float *gw = nullptr, *gb = nullptr, *loss = nullptr;
+    float* part = nullptr;  // gradient partials per tile (and warp), summed in a fixed order
     int* err = nullptr;
     uint16_t *w16 = nullptr, *x16 = nullptr, *h1 = nullptr, *h2 = nullptr, *g1 = nullptr, *g2 = nullptr,
              *dz3 = nullptr, *dz2 = nullptr, *dz1 = nullptr;
@@ -550,6 +568,8 @@ MlpTrainer* mlp_trainer_create(int max_batch, const float* w32, const float* b32
     A((void**)&t->dz3, sizeof(uint16_t) * cap * 64);
     A((void**)&t->dz2, sizeof(uint16_t) * cap * 64);
     A((void**)&t->dz1, sizeof(uint16_t) * cap * 64);
+    const size_t tiles = (cap + TILE - 1) / TILE;
+    A((void**)&t->part, sizeof(float) * tiles * std::max<size_t>(64 * 64 + 64, 4 * FWD_PART));
     if (!ok) {
         mlp_trainer_destroy(t);
         return nullptr;
@@ -567,7 +587,7 @@ MlpTrainer* mlp_trainer_create(int max_batch, const float* w32, const float* b32
 void mlp_trainer_destroy(MlpTrainer* t) {
     if (!t) return;
     void* ps[] = {t->w32, t->b32, t->mw, t->vw, t->mb, t->vb, t->gw, t->gb, t->loss, t->err, t->w16,
-                  t->x16, t->h1, t->h2, t->g1, t->g2, t->dz3, t->dz2, t->dz1};
+                  t->x16, t->h1, t->h2, t->g1, t->g2, t->dz3, t->dz2, t->dz1, t->part};
     for (void* p : ps)
         if (p) cudaFree(p);
     delete t;
@@ -604,17 +624,28 @@ int mlp_gradients(MlpTrainer* t, const float* feat, const float* target, int B, 
     f.g1 = t->g1;
     f.g2 = t->g2;
     f.dz3 = t->dz3;
-    f.gw = t->gw;
-    f.gb = t->gb;
-    f.loss = t->loss;
+    f.part = t->part;
     f.err = t->err;
     k_mlp_fwd<true><<<grid, 128, FWD_SMEM_TRAIN, st>>>(f);
-    BwdIO b3{t->dz3, t->h2, t->w16 + W3_OFF, t->g2, t->dz2, t->gw + W3_OFF, t->gb + B3_OFF, B, t->err};
+    // the output layer's sums: loss, db4, dw4 (each its own sum over the slots)
+    k_sum_parts<<<1, 64, 0, st>>>(t->part, tiles * 4, FWD_PART, 1, t->loss);
+    k_sum_parts<<<1, 64, 0, st>>>(t->part + 1, tiles * 4, FWD_PART, 1, t->gb + B4_OFF);
+    k_sum_parts<<<1, 64, 0, st>>>(t->part + 2, tiles * 4, FWD_PART, 64, t->gw + W4_OFF);
+    // hidden layers: dW then db of each, from its per-tile slots
+    auto layer_sums = [&](int kin, float* gw, float* gb) {
+        const int stride = 64 * kin + 64;
+        k_sum_parts<<<(64 * kin + 255) / 256, 256, 0, st>>>(t->part, tiles, stride, 64 * kin, gw);
+        k_sum_parts<<<1, 64, 0, st>>>(t->part + 64 * kin, tiles, stride, 64, gb);
+    };
+    BwdIO b3{t->dz3, t->h2, t->w16 + W3_OFF, t->g2, t->dz2, t->part, B, t->err};
     k_mlp_bwd<64><<<grid, 128, 128 * 64 * 2 + 128 * 128 * 2 + 80 * 128 * 2 + 64 * 64 * 2, st>>>(b3);
-    BwdIO b2{t->dz2, t->h1, t->w16 + W2_OFF, t->g1, t->dz1, t->gw + W2_OFF, t->gb + B2_OFF, B, t->err};
+    layer_sums(64, t->gw + W3_OFF, t->gb + B3_OFF);
+    BwdIO b2{t->dz2, t->h1, t->w16 + W2_OFF, t->g1, t->dz1, t->part, B, t->err};
     k_mlp_bwd<64><<<grid, 128, 128 * 64 * 2 + 128 * 128 * 2 + 80 * 128 * 2 + 64 * 64 * 2, st>>>(b2);
-    BwdIO b1{t->dz1, t->x16, t->w16 + W1_OFF, nullptr, nullptr, t->gw + W1_OFF, t->gb + B1_OFF, B, t->err};
+    layer_sums(64, t->gw + W2_OFF, t->gb + B2_OFF);
+    BwdIO b1{t->dz1, t->x16, t->w16 + W1_OFF, nullptr, nullptr, t->part, B, t->err};
     k_mlp_bwd<16><<<grid, 128, 128 * 64 * 2 + 128 * 128 * 2 + 32 * 128 * 2 + 16 * 64 * 2, st>>>(b1);
+    layer_sums(16, t->gw + W1_OFF, t->gb + B1_OFF);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

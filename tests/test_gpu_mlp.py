@@ -75,6 +75,26 @@ def test_training_reduces_loss():
     tr.close()
 
 
+def test_training_is_reproducible():
+    """The gradients are summed per tile and warp and then in a fixed order (no
+    floating-point atomics), so the same rows and seed give the same weights bit
+    for bit, and the same warm-started solver state after them."""
+    feat, target = random_rows(8192 + 300, 5)  # a partial last tile
+    ft, tt = torch.from_numpy(feat).cuda(), torch.from_numpy(target).cuda()
+    out = []
+    for _ in range(2):
+        tr, losses = learned.train(ft, tt, epochs=2, batch=2048, lr=3e-3, log_every=1)
+        w32, b32, w16 = tr.params()
+        tr.close()
+        out.append((w32, b32, w16, [l for _, l in losses]))
+    w_a, b_a, h_a, l_a = out[0]
+    w_b, b_b, h_b, l_b = out[1]
+    assert np.array_equal(w_a.view(np.uint32), w_b.view(np.uint32))
+    assert np.array_equal(b_a.view(np.uint32), b_b.view(np.uint32))
+    assert np.array_equal(h_a, h_b)
+    assert l_a == l_b
+
+
 def test_recording_features_changes_nothing():
     sc = scenes.dam_break(16, (40, 20, 20), stable=True, iterations=3)
     a = Solver(sc.para, sc.grid_space, sc.boundary, sc.ext())
