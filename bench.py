@@ -559,6 +559,7 @@ def _timed_errors(solver, steps, flush, stream, barrier, max_over_ranks):
 # with LEARN_COLLECT_ITERS Jacobi iterations per substep (the target is the total
 # lambda those iterations apply), and the trust region factor (0: none).
 LEARN_COLLECT_ITERS = 4
+LEARN_TRAIN_SEED = 1000  # scene seed of the training run (evaluation runs use the rank)
 LEARN_CLAMP = 16.0
 LEARN_FLOOR = 1
 LEARN_CORRECTIONS = 2
@@ -571,7 +572,8 @@ WARM_BLOCK = 256
 def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, plain, plain_batched) -> dict:
     """Learned lambda warm start. The MLP is trained here, on the GPU with the
     library's tensor-core kernels, from 2,000 substeps of the 262,144-particle dam
-    break run by the plain solver (2,048 random particles per substep), then used
+    break run by the plain solver from another lattice jitter than the runs it is
+    evaluated on (2,048 random particles per substep), then used
     with LEARN_CORRECTIONS corrections (lambda0 + plain iterations) on config 3
     (the same dam break) and on the 64-scene batch. Every speed-up is taken at
     the same max density error (the largest one-sided error of any particle after
@@ -583,7 +585,9 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
     from pbf_b200 import BatchSolver, Solver, autotune, learned, multigpu, scenes
     t0 = _t.perf_counter()
     ext_kw = plain["ext_kw"]
-    scc = scenes.config1(seed=rank, iterations=LEARN_COLLECT_ITERS)
+    # trained on the same dam break with another lattice jitter (seed), so the
+    # trajectories it is evaluated on below were not seen in training
+    scc = scenes.config1(seed=LEARN_TRAIN_SEED + rank, iterations=LEARN_COLLECT_ITERS)
     feat, target = learned.collect(scc, substeps=2000, rows_per_substep=2048, seed=rank, ext=ext_kw)
     t1 = _t.perf_counter()
     tr, losses = learned.train(feat, target, epochs=3, batch=4096, lr=2e-3, log_every=500)
@@ -594,7 +598,8 @@ def measure_learned(args, rank, world, flush, stream, barrier, max_over_ranks, p
     out = {"training": {"substeps": 2000, "collect_iterations": LEARN_COLLECT_ITERS, "rows": 2000 * 2048,
                         "epochs": 3, "batch": 4096, "loss_first": losses[0][1], "loss_last": losses[-1][1],
                         "collect_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2)},
-           "corrections": LEARN_CORRECTIONS, "warm_clamp": LEARN_CLAMP, "warm_floor": LEARN_FLOOR}
+           "corrections": LEARN_CORRECTIONS, "warm_clamp": LEARN_CLAMP, "warm_floor": LEARN_FLOOR,
+           "train_scene_seed": LEARN_TRAIN_SEED + rank}
 
     # The fused warm pass stages the network's weights once per block and runs
     # 128-row MMA tiles: warm-started solvers take 256-thread blocks, one block
