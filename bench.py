@@ -560,7 +560,7 @@ def _timed_errors(solver, steps, flush, stream, barrier, max_over_ranks):
 # lambda those iterations apply), and the trust region factor (0: none).
 LEARN_COLLECT_ITERS = 4
 LEARN_TRAIN_SEED = 1000  # scene seed of the training run (evaluation runs use the rank)
-LEARN_CLAMP = 16.0
+LEARN_CLAMP = 32.0
 LEARN_FLOOR = 1
 LEARN_CORRECTIONS = 2
 # common max-error tolerances at which both solvers run adaptively (each
