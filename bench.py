@@ -168,6 +168,15 @@ REF_SAMPLE = ("reference PBFSolver::solve (src/solver.cpp built from its sources
               "80x40x40, 4 iterations), with the reference's own formulas: it has no stable mode")
 
 
+def host_threads() -> int:
+    """Host threads this process may run on (its affinity mask; the machine's
+    count where the platform has no mask)."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def cpu_baseline(seconds: float = 12.0) -> dict:
     """The reference CPU solver (kind "reference"), or the oracle port when the
     reference could not be built, on a bounded sample of the same workload: the
@@ -178,7 +187,7 @@ def cpu_baseline(seconds: float = 12.0) -> dict:
     sc = scenes.config1(stable=False)
     if O.refcpu_available():
         ref = O.RefCpu(sc.para, sc.grid_space, dims=(80, 40, 40))
-        threads = os.cpu_count() or 1
+        threads = host_threads()
         ref.set_threads(threads)
         pos, vel = sc.pos, sc.vel
         steps, t0 = 0, time.perf_counter()
@@ -222,7 +231,7 @@ def run_reference(args) -> int:
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver not built (oracle/_ref missing)"}))
         return 0
     ref = O.RefCpu(sc.para, sc.grid_space, dims=(80, 40, 40))
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     ref.set_threads(threads)
     pos, vel = sc.pos, sc.vel
     for _ in range(args.warmup):
